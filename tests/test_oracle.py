@@ -1,0 +1,246 @@
+"""Pins the CPU oracle against HiRep's own tests for this path (CPU only).
+
+Each test restates one of the reference's self-checking programs, with the
+tolerance that program uses:
+  TestProgram/DiracOperator/check_diracoperator_1.c  gauge covariance      < 1e-14
+  TestProgram/DiracOperator/check_diracoperator_2.c  plane waves (free)    known answer
+  TestProgram/DiracOperator/check_diracoperator_3.c  hermiticity g5D^2     < 1e-14
+  TestProgram/DiracOperator/check_diracoperator_6.c  FP32 vs FP64 Dphi     < 1e-6
+  TestProgram/Inverters/check_inverters_1.c          cg_mshift, 6 shifts   true residual < err2
+  TestProgram/Inverters/check_inverters_6.c          cg_mshift_flt vs cg   < 10 err2
+plus the geometry walk (first even sites of the serial 8^4 walk as printed by a
+probe of the reference build) and the autosun generator conventions.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from hirep_b200 import fields as F
+
+REPS = [(3, O.FUND), (2, O.ADJ), (3, O.SYM), (4, O.ASYM), (2, O.FUND), (3, O.ADJ)]
+
+
+def _setup(dims, ng, rep, seed=1, smooth=None, bc=True):
+    o = O.Oracle(*dims, ng, rep)
+    u = F.hot_gauge(seed, o.V, ng) if smooth is None else F.smooth_gauge(seed, o.V, ng, smooth)
+    uf = o.represent_gauge_field(u, bc)
+    o.set_gauge(uf)
+    return o, u, uf
+
+
+def test_geometry_walk_pins():
+    o = O.Oracle(8, 8, 8, 8, 3, O.FUND)
+    ipt, iup, idn = o.geometry()
+    V = o.V
+    # serial walk puts even sites first and odd sites second
+    coords = {}
+    for t in range(8):
+        for x in range(8):
+            for y in range(8):
+                for z in range(8):
+                    ix = ipt[((t * 8 + x) * 8 + y) * 8 + z]
+                    coords[ix] = (t, x, y, z)
+                    assert (ix < V // 2) == ((t + x + y + z) % 2 == 0)
+    assert sorted(coords) == list(range(V))
+    # first even sites of the reference walk on 8^4: (0,0,0,0), (0,1,1,0), (0,1,0,1)
+    assert coords[0] == (0, 0, 0, 0)
+    assert coords[1] == (0, 1, 1, 0)
+    assert coords[2] == (0, 1, 0, 1)
+    # neighbours (check_geometry_1 style)
+    for ix in range(V):
+        c = coords[ix]
+        for mu in range(4):
+            up = list(c)
+            up[mu] = (up[mu] + 1) % 8
+            assert coords[iup[4 * ix + mu]] == tuple(up)
+            assert idn[4 * iup[4 * ix + mu] + mu] == ix
+
+
+@pytest.mark.parametrize("ng,rep", REPS)
+def test_representation_conventions(ng, rep):
+    o = O.Oracle(2, 2, 2, 2, ng, rep)
+    rng = np.random.default_rng(3)
+    u = F.haar_su_n(rng, 2, ng)
+    Ra, Rb, Rab = (o.group_represent(m) for m in (u[0], u[1], u[0] @ u[1]))
+    assert np.abs(Ra @ Rb - Rab).max() < 1e-13
+    assert np.abs(Ra @ Ra.conj().T - np.eye(o.nf)).max() < 1e-13
+    gT, rT, norms = o.generators()
+    assert norms[0] == 0.5
+    expect = {O.FUND: 0.5, O.ADJ: ng, O.SYM: (ng + 2) / 2, O.ASYM: (ng - 2) / 2}[rep]
+    assert norms[1] == pytest.approx(expect)
+    # Tr T_A T_B = delta_AB / 2
+    tr = np.einsum("aij,bji->ab", gT, gT)
+    assert np.abs(tr - 0.5 * np.eye(o.dimg)).max() < 1e-14
+    # R(exp(eps X)) = 1 + eps R(X) + O(eps^2): _group_represent2 agrees with the generators
+    h = rng.standard_normal(o.dimg)
+    eps = 1e-6
+    Xf = np.einsum("a,aij->ij", h, 1j * gT)
+    Xr = np.einsum("a,aij->ij", h, rT)
+    E = F.exp_i_hermitian((-1j * eps * Xf)[None])[0]
+    assert np.abs((o.group_represent(E) - np.eye(o.nf)) / eps - Xr).max() < 1e-5
+    assert np.abs(o.algebra_project(Xr.real if o.real else Xr) - h).max() < 1e-13
+
+
+def _plane_wave_case(o, rng, hmass):
+    T, X, Y, Z = o.dims
+    ipt, _, _ = o.geometry()
+    n = [rng.integers(0, L) for L in (T, X, Y, Z)]
+    p = [2 * np.pi * n[k] / L for k, L in enumerate((T, X, Y, Z))]
+    s = rng.standard_normal((4, o.nf)) + 1j * rng.standard_normal((4, o.nf))
+    psi = np.zeros((o.V, 4, o.nf), complex)
+    tt, xx, yy, zz = np.meshgrid(range(T), range(X), range(Y), range(Z), indexing="ij")
+    ph = np.exp(1j * (p[0] * tt + p[1] * xx + p[2] * yy + p[3] * zz))
+    psi[ipt.reshape(T, X, Y, Z)] = ph[..., None, None] * s
+    mp = hmass + sum(1 - np.cos(q) for q in p)
+    expect = mp * psi
+    for mu in range(4):
+        expect = expect + 1j * np.sin(p[mu]) * o.gamma(mu, psi)
+    return psi, expect
+
+
+def test_plane_waves_free_field():
+    """check_diracoperator_2: Dphi on plane waves, unit links, periodic BCs."""
+    for ng, rep in [(3, O.FUND), (2, O.ADJ)]:
+        o = O.Oracle(4, 4, 4, 4, ng, rep)
+        unit = np.broadcast_to(np.eye(ng, dtype=complex), (o.V, 4, ng, ng)).copy()
+        o.set_gauge(o.represent_gauge_field(unit, bc_t_antiperiodic=False))
+        rng = np.random.default_rng(7)
+        for _ in range(5):
+            psi, expect = _plane_wave_case(o, rng, 0.1)
+            got = o.Dphi(0.1, psi)
+            assert np.abs(got - expect).max() < 1e-13 * np.abs(expect).max() + 1e-14
+
+
+def _gauge_transform(o, u, g):
+    """U'(x,mu) = g(x) U(x,mu) g(x+mu)^+ on fundamental links."""
+    _, iup, _ = o.geometry()
+    up = np.empty_like(u)
+    for mu in range(4):
+        gy = g[iup[mu::4]]
+        up[:, mu] = g @ u[:, mu] @ np.conj(np.swapaxes(gy, 1, 2))
+    return up
+
+
+@pytest.mark.parametrize("ng,rep", REPS)
+def test_gauge_covariance(ng, rep):
+    """check_diracoperator_1: ||D[U^g](g psi) - g D[U] psi|| < 1e-14 (normalised psi)."""
+    o, u, uf = _setup((4, 4, 4, 4), ng, rep, seed=11)
+    psi = F.gaussian_spinor(5, o.V, o.nf)
+    psi /= np.sqrt(o.sqnorm(psi))
+    d1 = o.Dphi(0.1, psi)
+    g = F.haar_su_n(np.random.default_rng(9), o.V, ng)
+    Rg = np.stack([o.group_represent(m) for m in g])
+    o.set_gauge(o.represent_gauge_field(_gauge_transform(o, u, g), True))
+    gpsi = np.einsum("xij,xsj->xsi", Rg, psi)
+    d2 = o.Dphi(0.1, gpsi)
+    diff = d2 - np.einsum("xij,xsj->xsi", Rg, d1)
+    assert np.sqrt(o.sqnorm(diff)) < 1e-14 * 10
+
+
+@pytest.mark.parametrize("ng,rep", REPS)
+def test_hermiticity_eopre_sq(ng, rep):
+    """check_diracoperator_3: <a, g5D_eo^2 b> = <g5D_eo^2 a, b>."""
+    o, _, _ = _setup((4, 4, 4, 4), ng, rep, seed=2)
+    a = F.gaussian_spinor(1, o.VH, o.nf)
+    b = F.gaussian_spinor(2, o.VH, o.nf)
+    Ma, Mb = o.g5Dphi_eopre_sq(0.1, a), o.g5Dphi_eopre_sq(0.1, b)
+    lhs = np.vdot(a, Mb)
+    rhs = np.vdot(Ma, b)
+    assert abs(lhs - rhs) / abs(lhs) < 1e-14 * 10
+    # g5 D is hermitian on the full lattice
+    a = F.gaussian_spinor(3, o.V, o.nf)
+    b = F.gaussian_spinor(4, o.V, o.nf)
+    assert abs(np.vdot(a, o.g5Dphi(0.2, b)) - np.vdot(o.g5Dphi(0.2, a), b)) < 1e-11
+
+
+def test_eopre_schur_complement():
+    """Dphi_eopre = (4+m)^2 - D_eo D_oe on even sites, checked against the full operator."""
+    o, _, _ = _setup((4, 4, 4, 4), 3, O.FUND, seed=4)
+    m = -0.3
+    e = F.gaussian_spinor(6, o.VH, o.nf)
+    full = np.zeros((o.V, 4, o.nf), complex)
+    full[: o.VH] = e
+    # D_oe e, then D_eo of it, using the full-lattice hopping term
+    h1 = o.Dphi_(full, O.FULL, O.FULL)
+    h1[: o.VH] = 0
+    h2 = o.Dphi_(h1, O.FULL, O.FULL)[: o.VH]
+    expect = (4 + m) ** 2 * e - h2
+    got = o.Dphi_eopre(m, e)
+    assert np.abs(got - expect).max() < 1e-12
+
+
+def test_float_vs_double_dphi():
+    """check_diracoperator_6: FP32 Dphi agrees with FP64 to 1e-6 (relative norm)."""
+    o, _, _ = _setup((4, 4, 4, 4), 3, O.FUND, seed=5)
+    psi = F.gaussian_spinor(3, o.V, o.nf)
+    d = o.Dphi(0.1, psi)
+    f = o.Dphi_flt(0.1, psi.astype(np.complex64))
+    assert np.sqrt(o.sqnorm(d - f) / o.sqnorm(d)) < 1e-6
+
+
+def test_cg_mshift_six_shifts():
+    """check_inverters_1: 6 shifts on g5Dphi_sq(-0.1), each true residual < err2."""
+    o, _, _ = _setup((4, 4, 4, 4), 3, O.FUND, seed=6)
+    o.set_mass(-0.1)
+    shifts = [0.1, -0.21, 0.05, -0.01, -0.15, -0.05]
+    err2 = 1e-28
+    b = F.gaussian_spinor(8, o.V, o.nf) / np.sqrt(2.0)
+    out, it = o.cg_mshift(O.OP_G5DPHI_SQ, shifts, err2, b)
+    assert it > 0
+    for i, s in enumerate(shifts):
+        r = o.g5Dphi_sq(-0.1, out[i]) - s * out[i] - b
+        assert o.sqnorm(r) / o.sqnorm(b) < err2
+
+
+def test_cg_mshift_flt_vs_double():
+    """check_inverters_6: mixed precision vs double on g5Dphi_eopre_sq(-1.2), err2 1e-20."""
+    o, _, _ = _setup((4, 4, 4, 4), 3, O.FUND, seed=7)
+    o.set_mass(-1.2)
+    shifts = [-0.0, -0.1, -0.2, 0.1, 0.2, 0.3]
+    err2 = 1e-20
+    b = F.gaussian_spinor(9, o.VH, o.nf)
+    x_f, _ = o.cg_mshift(O.OP_G5DPHI_EOPRE_SQ, shifts, err2, b, flt=True)
+    x_d, _ = o.cg_mshift(O.OP_G5DPHI_EOPRE_SQ, shifts, err2, b)
+    for i, s in enumerate(shifts):
+        for x in (x_f[i], x_d[i]):
+            r = o.g5Dphi_eopre_sq(-1.2, x) - s * x - b
+            assert o.sqnorm(r) / o.sqnorm(b) < err2
+        r = o.g5Dphi_eopre_sq(-1.2, x_f[i] - x_d[i]) - s * (x_f[i] - x_d[i])
+        assert o.sqnorm(r) / o.sqnorm(b) < 10 * err2
+
+
+@pytest.mark.parametrize("ng,rep", [(3, O.FUND), (2, O.ADJ), (3, O.SYM)])
+def test_clover_inverse_and_hermiticity(ng, rep):
+    o, _, _ = _setup((4, 4, 4, 4), ng, rep, seed=12, smooth=0.3)
+    o.clover_init(1.0)
+    o.compute_clover_term()
+    m = -0.2
+    psi = F.gaussian_spinor(1, o.VH, o.nf)
+    back = o.Cphi_diag_inv(m, o.Cphi_diag(m, psi, O.ODD), O.ODD)
+    assert np.abs(back - psi).max() < 1e-13
+    a = F.gaussian_spinor(2, o.VH, o.nf)
+    b = F.gaussian_spinor(3, o.VH, o.nf)
+    lhs = np.vdot(a, o.g5Cphi_eopre_sq(m, b))
+    rhs = np.vdot(o.g5Cphi_eopre_sq(m, a), b)
+    assert abs(lhs - rhs) / abs(lhs) < 1e-13
+    # the clover term is hermitian in each chiral block
+    cl = o.clover_term()
+    for blk in (0, 2):
+        assert np.abs(cl[:, blk] - np.conj(np.swapaxes(cl[:, blk], 1, 2))).max() < 1e-14
+    # clover eopre is the Schur complement of the full clover operator
+    full = np.zeros((o.V, 4, o.nf), complex)
+    full[: o.VH] = psi
+    h = o.Dphi_(full, O.FULL, O.FULL)
+    h[: o.VH] = 0
+    h[o.VH:] = o.Cphi_diag_inv(m, h[o.VH:], O.ODD)
+    h2 = o.Dphi_(h, O.FULL, O.FULL)[: o.VH]
+    expect = o.Cphi_diag(m, psi, O.EVEN) - h2
+    assert np.abs(o.Cphi_eopre(m, psi) - expect).max() < 1e-12
+
+
+def test_smooth_field_plaquette():
+    """exp(i 0.3 H) links give an average plaquette near 0.8 (config 2's field)."""
+    o = O.Oracle(4, 4, 4, 4, 3, O.FUND)
+    u = F.smooth_gauge(7, o.V, 3, 0.3)
+    p = o.avr_plaquette(u)
+    assert 0.7 < p < 0.9
