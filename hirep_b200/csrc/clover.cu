@@ -1,0 +1,358 @@
+// clover.cu -- clover term on the device (LibHR/Update/clover_tools.c).
+//
+// The clover term A (four NF x NF blocks s0..s3 per site, clover_tools.c:161-206)
+// is built from the four-leaf loops.  For the operators it is repacked as two
+// Hermitian 2NF x 2NF blocks per site,
+//   block 0 = [[s0, s1], [s1^+, -s0]] acting on spin (0,1)
+//   block 1 = [[s2, s3], [s3^+, -s2]] acting on spin (2,3)     (Dphi.c:1113-1131)
+// stored as packed lower triangles (real diagonal, complex strict lower part).
+// D = (4+m) + A is kept packed, and so is D^-1, computed in FP64 from HiRep's
+// LDL factorisation (clover_tools.c:97-159) followed by forward/back
+// substitution of unit vectors (as in _compute_clover_force, :208-250).  The
+// operators then apply D or D^-1 as a dense Hermitian mat-vec fused into the
+// hopping kernel's epilogue instead of a per-site triangular solve.
+#include "dirac.cuh"
+
+namespace hrgpu {
+
+static inline unsigned nb(long n, int t = 128) { return (unsigned)((n + t - 1) / t); }
+
+// four-leaf loop (clover_tools.c:59-95)
+template <int N, bool REAL>
+__device__ void clover_loop_dev(CMat<N> &u, const void *U, const Geo &g, long lp, int t, int x, int y, int z, int mu,
+                                int nu) {
+  CMat<N> a, b, s1, s2, s3;
+  long id = ((t + x + y + z) & 1) * g.ld + coords_to_cb(g, t, x, y, z);
+  // leaf 1
+  long o1 = nbr_index(g, t, x, y, z, mu, +1), o2 = nbr_index(g, t, x, y, z, nu, +1);
+  mload<N, REAL>(a, U, mu, id, lp); mload<N, REAL>(b, U, nu, o1, lp); mmul<N, false, false>(s1, a, b);
+  mload<N, REAL>(a, U, nu, id, lp); mload<N, REAL>(b, U, mu, o2, lp); mmul<N, false, false>(s2, a, b);
+  mmul<N, false, true>(u, s1, s2);
+  // leaf 2: o1 = x-mu, o2 = x-mu+nu
+  int tt = t, xx = x, yy = y, zz = z;
+  {
+    int c[4] = {t, x, y, z};
+    c[mu] = (c[mu] - 1 + (mu == 0 ? g.T : mu == 1 ? g.X : mu == 2 ? g.Y : g.Z)) % (mu == 0 ? g.T : mu == 1 ? g.X : mu == 2 ? g.Y : g.Z);
+    tt = c[0]; xx = c[1]; yy = c[2]; zz = c[3];
+  }
+  o1 = nbr_index(g, t, x, y, z, mu, -1);
+  o2 = nbr_index(g, tt, xx, yy, zz, nu, +1);
+  mload<N, REAL>(a, U, nu, o1, lp); mload<N, REAL>(b, U, mu, o2, lp); mmul<N, false, false>(s1, a, b);
+  mload<N, REAL>(a, U, nu, id, lp); mmul<N, false, true>(s2, a, s1);
+  mload<N, REAL>(a, U, mu, o1, lp); mmul<N, false, false>(s3, s2, a);
+  madd(u, s3);
+  // leaf 3: o1 = x-mu, o2 = x-nu, o3 = x-mu-nu
+  long o3 = nbr_index(g, tt, xx, yy, zz, nu, -1);
+  o2 = nbr_index(g, t, x, y, z, nu, -1);
+  mload<N, REAL>(a, U, nu, o3, lp); mload<N, REAL>(b, U, mu, o1, lp); mmul<N, false, false>(s1, a, b);
+  mload<N, REAL>(a, U, mu, o3, lp); mmul<N, true, false>(s2, s1, a);
+  mload<N, REAL>(a, U, nu, o2, lp); mmul<N, false, false>(s3, s2, a);
+  madd(u, s3);
+  // leaf 4: o1 = x-nu, o2 = x-nu+mu
+  {
+    int c[4] = {t, x, y, z};
+    c[nu] = (c[nu] - 1 + (nu == 0 ? g.T : nu == 1 ? g.X : nu == 2 ? g.Y : g.Z)) % (nu == 0 ? g.T : nu == 1 ? g.X : nu == 2 ? g.Y : g.Z);
+    tt = c[0]; xx = c[1]; yy = c[2]; zz = c[3];
+  }
+  o1 = nbr_index(g, t, x, y, z, nu, -1);
+  o2 = nbr_index(g, tt, xx, yy, zz, mu, +1);
+  mload<N, REAL>(a, U, nu, o1, lp); mload<N, REAL>(b, U, mu, o1, lp); mmul<N, true, false>(s1, a, b);
+  mload<N, REAL>(a, U, nu, o2, lp); mload<N, REAL>(b, U, mu, id, lp); mmul<N, false, true>(s2, a, b);
+  mmul<N, false, false>(s3, s1, s2);
+  madd(u, s3);
+}
+
+// compute_clover_term (clover_tools.c:161-206)
+template <int N, bool REAL>
+__global__ void k_clover_term(double2 *cl, const void *U, Geo g, double csw) {
+  long d = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= 2L * g.ld) return;
+  int p = d >= g.ld ? 1 : 0;
+  if (d - p * g.ld >= g.VH) return;
+  int t, x, y, z;
+  dev_coords(g, (int)d, t, x, y, z);
+  const long lp = 2L * g.ld;
+  CMat<N> tmp[6];
+  clover_loop_dev<N, REAL>(tmp[0], U, g, lp, t, x, y, z, 0, 1);
+  clover_loop_dev<N, REAL>(tmp[1], U, g, lp, t, x, y, z, 0, 2);
+  clover_loop_dev<N, REAL>(tmp[2], U, g, lp, t, x, y, z, 0, 3);
+  clover_loop_dev<N, REAL>(tmp[3], U, g, lp, t, x, y, z, 1, 2);
+  clover_loop_dev<N, REAL>(tmp[4], U, g, lp, t, x, y, z, 1, 3);
+  clover_loop_dev<N, REAL>(tmp[5], U, g, lp, t, x, y, z, 2, 3);
+  const double c = -csw / 16.0;
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < N; j++) {
+      int ij = i * N + j, ji = j * N + i;
+      double2 at, bt, ct, dt;
+      if (REAL) {
+        // real loops: at = i(t2_ji - t2_ij), bt = i(t3_ij - t3_ji), ct = t1_ji - t1_ij + i(t0_ji - t0_ij),
+        // dt = t4_ij - t4_ji + i(t5_ji - t5_ij)
+        at = make_double2(0.0, tmp[2].c[ji].x - tmp[2].c[ij].x);
+        bt = make_double2(0.0, tmp[3].c[ij].x - tmp[3].c[ji].x);
+        ct = make_double2(tmp[1].c[ji].x - tmp[1].c[ij].x, tmp[0].c[ji].x - tmp[0].c[ij].x);
+        dt = make_double2(tmp[4].c[ij].x - tmp[4].c[ji].x, tmp[5].c[ji].x - tmp[5].c[ij].x);
+      } else {
+        double2 q;
+        // at = i (conj(t2_ji) - t2_ij)
+        q = make_double2(tmp[2].c[ji].x - tmp[2].c[ij].x, -tmp[2].c[ji].y - tmp[2].c[ij].y);
+        at = make_double2(-q.y, q.x);
+        q = make_double2(tmp[3].c[ij].x - tmp[3].c[ji].x, -tmp[3].c[ij].y - tmp[3].c[ji].y);
+        bt = make_double2(-q.y, q.x);
+        // ct = i (conj(t0_ji) - t0_ij) - t1_ij + conj(t1_ji)
+        q = make_double2(tmp[0].c[ji].x - tmp[0].c[ij].x, -tmp[0].c[ji].y - tmp[0].c[ij].y);
+        ct = make_double2(-q.y - tmp[1].c[ij].x + tmp[1].c[ji].x, q.x - tmp[1].c[ij].y - tmp[1].c[ji].y);
+        // dt = t4_ij - conj(t4_ji) + i (conj(t5_ji) - t5_ij)
+        q = make_double2(tmp[5].c[ji].x - tmp[5].c[ij].x, -tmp[5].c[ji].y - tmp[5].c[ij].y);
+        dt = make_double2(tmp[4].c[ij].x - tmp[4].c[ji].x - q.y, tmp[4].c[ij].y + tmp[4].c[ji].y + q.x);
+      }
+      double2 bc = make_double2(bt.x, -bt.y);  // conj(bt)
+      cl[((long)0 * N * N + ij) * lp + d] = make_double2(c * (at.x - bc.x), c * (at.y - bc.y));
+      cl[((long)1 * N * N + ij) * lp + d] = make_double2(c * (ct.x - dt.x), c * (ct.y - dt.y));
+      cl[((long)2 * N * N + ij) * lp + d] = make_double2(-c * (at.x + bc.x), -c * (at.y + bc.y));
+      cl[((long)3 * N * N + ij) * lp + d] = make_double2(-c * (ct.x + dt.x), -c * (ct.y + dt.y));
+    }
+}
+
+// Hermitian block b (0: s0,s1; 1: s2,s3) plus sigma on the diagonal, element (i,j), i >= j
+template <int N>
+__device__ __forceinline__ double2 hblock(const double2 *cl, int b, int i, int j, long lp, long d, double sigma) {
+  const int N2 = N * N;
+  const double2 *sa = cl + (long)(2 * b) * N2 * lp + d, *sb = cl + (long)(2 * b + 1) * N2 * lp + d;
+  double2 v;
+  if (i < N) {
+    v = __ldg(sa + (long)(i * N + j) * lp);
+  } else if (j < N) {
+    double2 s = __ldg(sb + (long)(j * N + (i - N)) * lp);
+    v = make_double2(s.x, -s.y);
+  } else {
+    double2 s = __ldg(sa + (long)((i - N) * N + (j - N)) * lp);
+    v = make_double2(-s.x, -s.y);
+  }
+  if (i == j) v.x += sigma;
+  return v;
+}
+
+template <int N>
+__global__ void k_clover_pack_diag(const double2 *cl, double sigma, double *dg, double2 *od, Geo g) {
+  long d = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= 2L * g.ld) return;
+  const long lp = 2L * g.ld;
+  const int n = 2 * N;
+  for (int b = 0; b < 2; b++) {
+    for (int i = 0; i < n; i++) dg[((long)b * n + i) * lp + d] = hblock<N>(cl, b, i, i, lp, d, sigma).x;
+    for (int i = 1; i < n; i++)
+      for (int j = 0; j < i; j++)
+        od[((long)b * N * (2 * N - 1) + i * (i - 1) / 2 + j) * lp + d] = hblock<N>(cl, b, i, j, lp, d, sigma);
+  }
+}
+
+// LDL (clover_tools.c:97-114) and explicit inverse, packed
+template <int N>
+__global__ void k_clover_pack_inv(const double2 *cl, double sigma, double *dg, double2 *od, Geo g) {
+  long d = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= 2L * g.ld) return;
+  int p = d >= g.ld ? 1 : 0;
+  const long lp = 2L * g.ld;
+  constexpr int n = 2 * N;
+  if (d - p * g.ld >= g.VH) {
+    for (int b = 0; b < 2; b++) {
+      for (int i = 0; i < n; i++) dg[((long)b * n + i) * lp + d] = 0.0;
+      for (int k = 0; k < N * (2 * N - 1); k++) od[((long)b * N * (2 * N - 1) + k) * lp + d] = make_double2(0.0, 0.0);
+    }
+    return;
+  }
+  double2 A[n * (n + 1) / 2];
+  double2 col[n];
+#define CP(i, j) A[(i) * ((i) + 1) / 2 + (j)]
+  for (int b = 0; b < 2; b++) {
+    for (int i = 0; i < n; i++)
+      for (int j = 0; j <= i; j++) CP(i, j) = hblock<N>(cl, b, i, j, lp, d, sigma);
+    for (int i = 0; i < n; i++) {
+      for (int k = 0; k < i; k++) {
+        double2 a = CP(i, k);
+        double w = (a.x * a.x + a.y * a.y) * CP(k, k).x;
+        CP(i, i).x -= w;  // conj(a) a D_k is real
+      }
+      for (int j = i + 1; j < n; j++) {
+        for (int k = 0; k < i; k++) {
+          double2 a = CP(i, k), c = CP(j, k);
+          // conj(a) * c * D_k
+          double2 q = make_double2((a.x * c.x + a.y * c.y) * CP(k, k).x, (a.x * c.y - a.y * c.x) * CP(k, k).x);
+          CP(j, i) = csub(CP(j, i), q);
+        }
+        double di = CP(i, i).x;
+        CP(j, i) = make_double2(CP(j, i).x / di, CP(j, i).y / di);
+      }
+    }
+    for (int c = 0; c < n; c++) {
+      for (int i = 0; i < n; i++) col[i] = make_double2(i == c ? 1.0 : 0.0, 0.0);
+      for (int i = c; i < n; i++)
+        for (int k = 0; k < i; k++) {
+          double2 l = CP(i, k), v = col[k];
+          col[i] = make_double2(col[i].x - (l.x * v.x - l.y * v.y), col[i].y - (l.x * v.y + l.y * v.x));
+        }
+      for (int i = n - 1; i >= c; i--) {
+        double di = CP(i, i).x;
+        col[i] = make_double2(col[i].x / di, col[i].y / di);
+        for (int k = i + 1; k < n; k++) {
+          double2 l = CP(k, i), v = col[k];  // conj(l) * v
+          col[i] = make_double2(col[i].x - (l.x * v.x + l.y * v.y), col[i].y - (l.x * v.y - l.y * v.x));
+        }
+      }
+      dg[((long)b * n + c) * lp + d] = col[c].x;
+      for (int i = c + 1; i < n; i++) od[((long)b * N * (2 * N - 1) + i * (i - 1) / 2 + c) * lp + d] = col[i];
+    }
+  }
+#undef CP
+}
+
+template <typename DST, typename SRC>
+__global__ void k_cvt(DST *dst, const SRC *src, long n) {
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = (DST)src[i];
+}
+
+// standalone Cphi_diag / Cphi_diag_inv on one parity (aliasing allowed)
+template <int N, typename R>
+__global__ void k_clover_apply(typename C2<R>::T *out, const typename C2<R>::T *in, const R *dg,
+                               const typename C2<R>::T *od, int p, Geo g) {
+  typedef typename C2<R>::T V;
+  int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cb >= g.VH) return;
+  const long ld = g.ld, lp = 2L * g.ld, site = (long)p * g.ld + cb;
+  V x[2 * N], y[2 * N];
+  V res[4 * N];
+  for (int b = 0; b < 2; b++) {
+    for (int i = 0; i < 2 * N; i++) x[i] = in[(long)(2 * b * N + i) * ld + cb];
+    herm_apply<N>(y, x, dg + (long)b * 2 * N * lp, od + (long)b * N * (2 * N - 1) * lp, lp, site, N);
+    for (int i = 0; i < 2 * N; i++) res[2 * b * N + i] = y[i];
+  }
+  for (int k = 0; k < 4 * N; k++) out[(long)k * ld + cb] = res[k];
+}
+
+}  // namespace hrgpu
+
+using namespace hrgpu;
+
+namespace hrgpu {
+
+static int alloc_clover() {
+  const long lp = 2L * L.ld;
+  const int n = 2 * L.nf, no = L.nf * (2 * L.nf - 1), n2 = L.nf * L.nf;
+  if (!L.cl_term) {
+    HR_CUDA(cudaMalloc(&L.cl_term, sizeof(double2) * 4 * n2 * lp));
+    HR_CUDA(cudaMemsetAsync(L.cl_term, 0, sizeof(double2) * 4 * n2 * lp, L.stream));
+    HR_CUDA(cudaMalloc(&L.cl_dg, sizeof(double) * 2 * n * lp));
+    HR_CUDA(cudaMalloc(&L.cl_od, sizeof(double2) * 2 * no * lp));
+    HR_CUDA(cudaMalloc(&L.cl_idg, sizeof(double) * 2 * n * lp));
+    HR_CUDA(cudaMalloc(&L.cl_iod, sizeof(double2) * 2 * no * lp));
+    HR_CUDA(cudaMalloc(&L.cl_dg_f, sizeof(float) * 2 * n * lp));
+    HR_CUDA(cudaMalloc(&L.cl_od_f, sizeof(float2) * 2 * no * lp));
+    HR_CUDA(cudaMalloc(&L.cl_idg_f, sizeof(float) * 2 * n * lp));
+    HR_CUDA(cudaMalloc(&L.cl_iod_f, sizeof(float2) * 2 * no * lp));
+    HR_CUDA(cudaMalloc(&L.cl_force, sizeof(double2) * 6 * n2 * lp));
+    HR_CUDA(cudaMemsetAsync(L.cl_force, 0, sizeof(double2) * 6 * n2 * lp, L.stream));
+  }
+  return 0;
+}
+
+int compute_clover_term_dev() {
+  HR_REQUIRE(L.clover, HRGPU_E_STATE, "compute_clover_term: clover not initialised");
+  if (int rc = check_gauge(HRGPU_DOUBLE)) return rc;
+  Geo g = make_geo();
+  long n = 2L * L.ld;
+  HR_NF_DISPATCH(L.real, L.nf, (k_clover_term<N_, R_><<<nb(n), 128, 0, L.stream>>>(L.cl_term, L.U, g, L.csw)));
+  HR_LAUNCH_CHECK();
+  L.sigma = 0xF00F;
+  L.sigma_diag = 0xF00F;
+  L.sigma_flt = 0xF00F;
+  return 0;
+}
+
+int clover_prepare(double mass, int prec) {
+  const double sigma = 4.0 + mass;
+  Geo g = make_geo();
+  long n = 2L * L.ld;
+  const long lp = 2L * L.ld;
+  if (L.sigma_diag != sigma) {
+    HR_NFC_DISPATCH(L.nf, (k_clover_pack_diag<N_><<<nb(n), 128, 0, L.stream>>>(L.cl_term, sigma, L.cl_dg, L.cl_od, g)));
+    HR_LAUNCH_CHECK();
+    L.sigma_diag = sigma;
+  }
+  if (L.sigma != sigma) {
+    HR_NFC_DISPATCH(L.nf, (k_clover_pack_inv<N_><<<nb(n), 64, 0, L.stream>>>(L.cl_term, sigma, L.cl_idg, L.cl_iod, g)));
+    HR_LAUNCH_CHECK();
+    L.sigma = sigma;
+  }
+  if (prec == HRGPU_FLOAT && L.sigma_flt != sigma) {
+    const long nd = 2L * 2 * L.nf * lp, no = 2L * L.nf * (2 * L.nf - 1) * lp * 2;
+    k_cvt<float, double><<<nb(nd, 256), 256, 0, L.stream>>>(L.cl_dg_f, L.cl_dg, nd);
+    k_cvt<float, double><<<nb(no, 256), 256, 0, L.stream>>>((float *)L.cl_od_f, (const double *)L.cl_od, no);
+    k_cvt<float, double><<<nb(nd, 256), 256, 0, L.stream>>>(L.cl_idg_f, L.cl_idg, nd);
+    k_cvt<float, double><<<nb(no, 256), 256, 0, L.stream>>>((float *)L.cl_iod_f, (const double *)L.cl_iod, no);
+    HR_LAUNCH_CHECK();
+    L.sigma_flt = sigma;
+  }
+  return 0;
+}
+
+template <>
+void clover_blocks<double>(const double **ddg, const double2 **dod, const double **idg, const double2 **iod) {
+  *ddg = L.cl_dg; *dod = L.cl_od; *idg = L.cl_idg; *iod = L.cl_iod;
+}
+template <>
+void clover_blocks<float>(const float **ddg, const float2 **dod, const float **idg, const float2 **iod) {
+  *ddg = L.cl_dg_f; *dod = L.cl_od_f; *idg = L.cl_idg_f; *iod = L.cl_iod_f;
+}
+
+// which: 0 = D = (4+m)+A, 1 = D^-1
+int clover_apply(int which, double mass, void *out, const void *in, int par) {
+  HR_REQUIRE(L.ready && L.clover, HRGPU_E_STATE, "Cphi_diag: no clover term");
+  HR_REQUIRE(out && in && par >= 0 && par <= 2, HRGPU_E_ARG, "Cphi_diag: bad arguments");
+  if (int rc = clover_prepare(mass, HRGPU_DOUBLE)) return rc;
+  Geo g = make_geo();
+  const double *dg = which ? L.cl_idg : L.cl_dg;
+  const double2 *od = which ? L.cl_iod : L.cl_od;
+  for (int p = 0; p < 2; p++) {
+    if (par != HRGPU_FULL && par != p) continue;
+    size_t off = par == HRGPU_FULL ? (size_t)p * 4 * L.nf * L.ld : 0;
+    double2 *o = (double2 *)out + off;
+    const double2 *i = (const double2 *)in + off;
+    HR_NFC_DISPATCH(L.nf, (k_clover_apply<N_, double><<<nb(L.VH), 128, 0, L.stream>>>(o, i, dg, od, p, g)));
+    HR_LAUNCH_CHECK();
+  }
+  return 0;
+}
+
+int links_out(void *host, const void *dev, int nel, int elem_bytes, int ndir);
+
+}  // namespace hrgpu
+
+extern "C" {
+
+int hrgpu_clover_init(double csw) {
+  HR_REQUIRE(L.ready, HRGPU_E_STATE, "hrgpu_clover_init: lattice not initialised");
+  if (int rc = alloc_clover()) return rc;
+  L.clover = true;
+  L.csw = csw;
+  L.sigma = L.sigma_diag = L.sigma_flt = 0xF00F;
+  if (L.have_gauge) return compute_clover_term_dev();
+  return 0;
+}
+
+int hrgpu_compute_clover_term(void) { return compute_clover_term_dev(); }
+
+int hrgpu_compute_ldl_decomp(double sigma) {
+  HR_REQUIRE(L.ready && L.clover, HRGPU_E_STATE, "hrgpu_compute_ldl_decomp: no clover term");
+  return clover_prepare(sigma - 4.0, HRGPU_DOUBLE);
+}
+
+int hrgpu_clover_term_get(void *cl_host) {
+  HR_REQUIRE(L.ready && L.clover, HRGPU_E_STATE, "hrgpu_clover_term_get: no clover term");
+  return links_out(cl_host, L.cl_term, L.nf * L.nf, 16, 4);
+}
+
+int hrgpu_Cphi_diag(double mass, void *out, const void *in, int par) { return clover_apply(0, mass, out, in, par); }
+int hrgpu_Cphi_diag_inv(double mass, void *out, const void *in, int par) { return clover_apply(1, mass, out, in, par); }
+
+}  // extern "C"

@@ -1,0 +1,242 @@
+// dirac.cu -- Wilson / clover Dirac operators on the device (LibHR/Update/Dphi.c,
+// Dphi_flt.c, D_update.c), built from the fused hopping kernel in hop.cuh.
+#include "dirac.cuh"
+
+namespace hrgpu {
+
+static unsigned long g_mvm = 0;
+static double g_static_mass = 0.0;
+
+template <typename R>
+static const void *links() {
+  return sizeof(R) == 8 ? L.U : L.Uf;
+}
+
+// one hop onto parity outp with the given epilogue; fields are parity fields
+template <typename R>
+int hop(int outp, void *out, const void *in, int ep, double cacc, const void *aux, double caux, int g5, double *red,
+        const R *cdg, const typename C2<R>::T *cod) {
+  HopArgs<R> a;
+  a.in = in;
+  a.out = out;
+  a.U = links<R>();
+  a.aux = aux;
+  a.cdg = cdg;
+  a.cod = cod;
+  a.red = red;
+  a.cacc = (R)cacc;
+  a.caux = (R)caux;
+  a.outp = outp;
+  a.g5 = g5;
+  a.stop = L.cur_stop;
+  g_mvm++;
+  return launch_hop<R>(ep, a);
+}
+template int hop<double>(int, void *, const void *, int, double, const void *, double, int, double *, const double *,
+                         const double2 *);
+template int hop<float>(int, void *, const void *, int, double, const void *, double, int, double *, const float *,
+                        const float2 *);
+
+int check_gauge(int prec) {
+  HR_REQUIRE(L.ready, HRGPU_E_STATE, "lattice not initialised");
+  if (prec == HRGPU_DOUBLE) HR_REQUIRE(L.have_gauge, HRGPU_E_STATE, "no gauge field set");
+  else HR_REQUIRE(L.have_gauge_flt, HRGPU_E_STATE, "no float gauge field set");
+  return 0;
+}
+
+template <typename R>
+static size_t par_elems() {
+  return (size_t)4 * L.nf * L.ld;  // complex elements of one parity field
+}
+
+template <typename R>
+static inline void *par_ptr(void *f, int p) {
+  return (char *)f + (size_t)p * par_elems<R>() * sizeof(typename C2<R>::T);
+}
+template <typename R>
+static inline const void *par_ptr(const void *f, int p) {
+  return (const char *)f + (size_t)p * par_elems<R>() * sizeof(typename C2<R>::T);
+}
+
+// Dphi_ on parity or full fields
+template <typename R>
+int Dphi_hop(void *out, int out_par, const void *in) {
+  if (int rc = check_gauge(sizeof(R) == 8 ? HRGPU_DOUBLE : HRGPU_FLOAT)) return rc;
+  HR_REQUIRE(out && in && out != in, HRGPU_E_ARG, "Dphi_: input and output fields must be different");
+  HR_REQUIRE(out_par >= 0 && out_par <= 2, HRGPU_E_ARG, "Dphi_: bad parity");
+  if (out_par == HRGPU_FULL) {
+    for (int p = 0; p < 2; p++)
+      if (int rc = hop<R>(p, par_ptr<R>(out, p), par_ptr<R>(in, p ^ 1), EP_AXPY, -0.5, nullptr, 0.0, 0, nullptr,
+                          nullptr, nullptr))
+        return rc;
+    g_mvm++;  // a full-lattice application counts twice (Dphi.c:205-207)
+    return 0;
+  }
+  return hop<R>(out_par, out, in, EP_AXPY, -0.5, nullptr, 0.0, 0, nullptr, nullptr, nullptr);
+}
+
+// full lattice: out = -1/2 H in + (4+m) in, optionally gamma_5 (Dphi / g5Dphi)
+template <typename R>
+int Dphi_full(double m0, void *out, const void *in, int g5) {
+  if (int rc = check_gauge(sizeof(R) == 8 ? HRGPU_DOUBLE : HRGPU_FLOAT)) return rc;
+  HR_REQUIRE(out && in && out != in, HRGPU_E_ARG, "Dphi: input and output fields must be different");
+  for (int p = 0; p < 2; p++)
+    if (int rc = hop<R>(p, par_ptr<R>(out, p), par_ptr<R>(in, p ^ 1), EP_AXPY, -0.5, par_ptr<R>(in, p), 4.0 + m0, g5,
+                        nullptr, nullptr, nullptr))
+      return rc;
+  return 0;
+}
+
+// even-odd: out = (4+m)^2 in - D_pq D_qp in on parity p, optionally gamma_5
+template <typename R>
+int Dphi_eo(double m0, void *out, const void *in, int outp, int g5, double *red) {
+  if (int rc = check_gauge(sizeof(R) == 8 ? HRGPU_DOUBLE : HRGPU_FLOAT)) return rc;
+  HR_REQUIRE(out && in && out != in, HRGPU_E_ARG, "Dphi_eopre: input and output fields must be different");
+  void **tmp = sizeof(R) == 8 ? &L.tmp_o : &L.tmp_o_f;
+  if (int rc = ensure_tmp(tmp, spinor_bytes(HRGPU_EVEN, sizeof(R) == 8 ? HRGPU_DOUBLE : HRGPU_FLOAT))) return rc;
+  if (int rc = hop<R>(outp ^ 1, *tmp, in, EP_AXPY, -0.5, nullptr, 0.0, 0, nullptr, nullptr, nullptr)) return rc;
+  double rho = 4.0 + m0;
+  if (sizeof(R) == 4) {
+    float r = 4.f + (float)m0;
+    rho = (double)(r * r);
+  } else {
+    rho = rho * rho;
+  }
+  return hop<R>(outp, out, *tmp, EP_AXPY, 0.5, in, rho, g5, red, nullptr, nullptr);
+}
+
+template int Dphi_eo<double>(double, void *, const void *, int, int, double *);
+template int Dphi_eo<float>(double, void *, const void *, int, int, double *);
+
+// ------------------------------------------------------------------ clover
+template <typename R>
+int Cphi_eo(double mass, void *out, const void *in, int g5, double *red) {
+  if (int rc = check_gauge(sizeof(R) == 8 ? HRGPU_DOUBLE : HRGPU_FLOAT)) return rc;
+  HR_REQUIRE(L.clover, HRGPU_E_STATE, "Cphi_eopre: no clover term (hrgpu_clover_init)");
+  HR_REQUIRE(out && in && out != in, HRGPU_E_ARG, "Cphi_eopre: input and output fields must be different");
+  if (int rc = clover_prepare(mass, sizeof(R) == 8 ? HRGPU_DOUBLE : HRGPU_FLOAT)) return rc;
+  void **tmp = sizeof(R) == 8 ? &L.tmp_o : &L.tmp_o_f;
+  if (int rc = ensure_tmp(tmp, spinor_bytes(HRGPU_EVEN, sizeof(R) == 8 ? HRGPU_DOUBLE : HRGPU_FLOAT))) return rc;
+  const R *idg;
+  const typename C2<R>::T *iod;
+  const R *ddg;
+  const typename C2<R>::T *dod;
+  clover_blocks<R>(&ddg, &dod, &idg, &iod);
+  if (int rc = hop<R>(HRGPU_ODD, *tmp, in, EP_CLOV_INV, -0.5, nullptr, 0.0, 0, nullptr, idg, iod)) return rc;
+  return hop<R>(HRGPU_EVEN, out, *tmp, EP_CLOV, 0.5, in, 0.0, g5, red, ddg, dod);
+}
+template int Cphi_eo<double>(double, void *, const void *, int, double *);
+template int Cphi_eo<float>(double, void *, const void *, int, double *);
+
+static int Cphi_full(double mass, void *out, const void *in, int g5) {
+  if (int rc = check_gauge(HRGPU_DOUBLE)) return rc;
+  HR_REQUIRE(L.clover, HRGPU_E_STATE, "Cphi: no clover term (hrgpu_clover_init)");
+  HR_REQUIRE(out && in && out != in, HRGPU_E_ARG, "Cphi: input and output fields must be different");
+  if (int rc = clover_prepare(mass, HRGPU_DOUBLE)) return rc;
+  const double *idg, *ddg;
+  const double2 *iod, *dod;
+  clover_blocks<double>(&ddg, &dod, &idg, &iod);
+  for (int p = 0; p < 2; p++)
+    if (int rc = hop<double>(p, par_ptr<double>(out, p), par_ptr<double>(in, p ^ 1), EP_CLOV, -0.5,
+                             par_ptr<double>(in, p), 0.0, g5, nullptr, ddg, dod))
+      return rc;
+  return 0;
+}
+
+template <typename R>
+static int sq(int (*op)(double, void *, const void *, int), double m, void *out, const void *in, int par) {
+  void **tmp = par == HRGPU_FULL ? (sizeof(R) == 8 ? &L.tmp_full : &L.tmp_full_f) : (sizeof(R) == 8 ? &L.tmp_e : &L.tmp_e_f);
+  if (int rc = ensure_tmp(tmp, spinor_bytes(par, sizeof(R) == 8 ? HRGPU_DOUBLE : HRGPU_FLOAT))) return rc;
+  if (int rc = op(m, *tmp, in, 1)) return rc;
+  return op(m, out, *tmp, 1);
+}
+
+static int op_Dfull_d(double m, void *o, const void *i, int g5) { return Dphi_full<double>(m, o, i, g5); }
+static int op_Dfull_f(double m, void *o, const void *i, int g5) { return Dphi_full<float>(m, o, i, g5); }
+static int op_eo_d(double m, void *o, const void *i, int g5) { return Dphi_eo<double>(m, o, i, HRGPU_EVEN, g5, nullptr); }
+static int op_eo_f(double m, void *o, const void *i, int g5) { return Dphi_eo<float>(m, o, i, HRGPU_EVEN, g5, nullptr); }
+static int op_ceo_d(double m, void *o, const void *i, int g5) { return Cphi_eo<double>(m, o, i, g5, nullptr); }
+static int op_ceo_f(double m, void *o, const void *i, int g5) { return Cphi_eo<float>(m, o, i, g5, nullptr); }
+static int op_cfull_d(double m, void *o, const void *i, int g5) { return Cphi_full(m, o, i, g5); }
+
+// operator used by the inverters: M = op(mass) on fields of the returned parity
+int apply_op(int op, int prec, double mass, void *out, const void *in) {
+  if (prec == HRGPU_DOUBLE) {
+    switch (op) {
+      case HRGPU_OP_G5DPHI_SQ: return sq<double>(op_Dfull_d, mass, out, in, HRGPU_FULL);
+      case HRGPU_OP_G5DPHI_EOPRE_SQ: return sq<double>(op_eo_d, mass, out, in, HRGPU_EVEN);
+      case HRGPU_OP_G5CPHI_EOPRE_SQ: return sq<double>(op_ceo_d, mass, out, in, HRGPU_EVEN);
+      case HRGPU_OP_G5CPHI_SQ: return sq<double>(op_cfull_d, mass, out, in, HRGPU_FULL);
+    }
+  } else {
+    switch (op) {
+      case HRGPU_OP_G5DPHI_SQ: return sq<float>(op_Dfull_f, mass, out, in, HRGPU_FULL);
+      case HRGPU_OP_G5DPHI_EOPRE_SQ: return sq<float>(op_eo_f, mass, out, in, HRGPU_EVEN);
+      case HRGPU_OP_G5CPHI_EOPRE_SQ: return sq<float>(op_ceo_f, mass, out, in, HRGPU_EVEN);
+      default: break;
+    }
+  }
+  set_error("operator %d has no %s version", op, prec == HRGPU_DOUBLE ? "double" : "float");
+  return HRGPU_E_ARG;
+}
+
+int op_parity(int op) { return (op == HRGPU_OP_G5DPHI_SQ || op == HRGPU_OP_G5CPHI_SQ) ? HRGPU_FULL : HRGPU_EVEN; }
+
+double static_mass() { return g_static_mass; }
+
+}  // namespace hrgpu
+
+using namespace hrgpu;
+
+extern "C" {
+
+int hrgpu_Dphi_(void *out, int out_par, const void *in) { return Dphi_hop<double>(out, out_par, in); }
+int hrgpu_Dphi(double m0, void *out, const void *in) { return Dphi_full<double>(m0, out, in, 0); }
+int hrgpu_g5Dphi(double m0, void *out, const void *in) { return Dphi_full<double>(m0, out, in, 1); }
+int hrgpu_g5Dphi_sq(double m0, void *out, const void *in) { return sq<double>(op_Dfull_d, m0, out, in, HRGPU_FULL); }
+int hrgpu_Dphi_eopre(double m0, void *out, const void *in) { return Dphi_eo<double>(m0, out, in, HRGPU_EVEN, 0, nullptr); }
+int hrgpu_Dphi_oepre(double m0, void *out, const void *in) { return Dphi_eo<double>(m0, out, in, HRGPU_ODD, 0, nullptr); }
+int hrgpu_g5Dphi_eopre(double m0, void *out, const void *in) { return Dphi_eo<double>(m0, out, in, HRGPU_EVEN, 1, nullptr); }
+int hrgpu_g5Dphi_eopre_sq(double m0, void *out, const void *in) { return sq<double>(op_eo_d, m0, out, in, HRGPU_EVEN); }
+
+int hrgpu_Dphi_flt_(void *out, int out_par, const void *in) { return Dphi_hop<float>(out, out_par, in); }
+int hrgpu_Dphi_flt(double m0, void *out, const void *in) { return Dphi_full<float>(m0, out, in, 0); }
+int hrgpu_g5Dphi_flt(double m0, void *out, const void *in) { return Dphi_full<float>(m0, out, in, 1); }
+int hrgpu_g5Dphi_sq_flt(double m0, void *out, const void *in) { return sq<float>(op_Dfull_f, m0, out, in, HRGPU_FULL); }
+int hrgpu_Dphi_eopre_flt(double m0, void *out, const void *in) { return Dphi_eo<float>(m0, out, in, HRGPU_EVEN, 0, nullptr); }
+int hrgpu_g5Dphi_eopre_flt(double m0, void *out, const void *in) { return Dphi_eo<float>(m0, out, in, HRGPU_EVEN, 1, nullptr); }
+int hrgpu_g5Dphi_eopre_sq_flt(double m0, void *out, const void *in) { return sq<float>(op_eo_f, m0, out, in, HRGPU_EVEN); }
+
+unsigned long hrgpu_getMVM(void) {
+  unsigned long r = g_mvm >> 1;
+  g_mvm = 0;
+  return r;
+}
+
+int hrgpu_Cphi(double mass, void *out, const void *in) { return Cphi_full(mass, out, in, 0); }
+int hrgpu_g5Cphi(double mass, void *out, const void *in) { return Cphi_full(mass, out, in, 1); }
+int hrgpu_g5Cphi_sq(double mass, void *out, const void *in) { return sq<double>(op_cfull_d, mass, out, in, HRGPU_FULL); }
+int hrgpu_Cphi_eopre(double mass, void *out, const void *in) { return Cphi_eo<double>(mass, out, in, 0, nullptr); }
+int hrgpu_g5Cphi_eopre(double mass, void *out, const void *in) { return Cphi_eo<double>(mass, out, in, 1, nullptr); }
+int hrgpu_g5Cphi_eopre_sq(double mass, void *out, const void *in) { return sq<double>(op_ceo_d, mass, out, in, HRGPU_EVEN); }
+int hrgpu_g5Cphi_eopre_flt(double mass, void *out, const void *in) { return Cphi_eo<float>(mass, out, in, 1, nullptr); }
+int hrgpu_g5Cphi_eopre_sq_flt(double mass, void *out, const void *in) { return sq<float>(op_ceo_f, mass, out, in, HRGPU_EVEN); }
+
+int hrgpu_set_dirac_mass(double mass) {
+  g_static_mass = mass;
+  return 0;
+}
+double hrgpu_get_dirac_mass(void) { return g_static_mass; }
+
+// H2, H, D of D_update.c:41-95 in the UPDATE_EO build
+int hrgpu_H2(void *out, const void *in) {
+  return L.clover ? hrgpu_g5Cphi_eopre_sq(g_static_mass, out, in) : hrgpu_g5Dphi_eopre_sq(g_static_mass, out, in);
+}
+int hrgpu_H(void *out, const void *in) {
+  return L.clover ? hrgpu_g5Cphi_eopre(g_static_mass, out, in) : hrgpu_g5Dphi_eopre(g_static_mass, out, in);
+}
+int hrgpu_D(void *out, const void *in) {
+  return L.clover ? hrgpu_Cphi_eopre(g_static_mass, out, in) : hrgpu_Dphi_eopre(g_static_mass, out, in);
+}
+
+}  // extern "C"

@@ -1,0 +1,130 @@
+// dirac.cuh -- internal interfaces between the operator, clover, inverter and
+// force translation units.
+#pragma once
+#include "hop.cuh"
+
+namespace hrgpu {
+
+template <typename R>
+int launch_hop(int ep, HopArgs<R> &a);
+
+template <typename R>
+int hop(int outp, void *out, const void *in, int ep, double cacc, const void *aux, double caux, int g5, double *red,
+        const R *cdg, const typename C2<R>::T *cod);
+
+int check_gauge(int prec);
+template <typename R>
+int Dphi_eo(double m0, void *out, const void *in, int outp, int g5, double *red);
+template <typename R>
+int Cphi_eo(double mass, void *out, const void *in, int g5, double *red);
+int apply_op(int op, int prec, double mass, void *out, const void *in);
+int op_parity(int op);
+double static_mass();
+
+// clover: make sure the packed (4+m)+A blocks and their inverse exist for this
+// mass in this precision (the LDL cache of clover_tools.c:343-358)
+int clover_prepare(double mass, int prec);
+template <typename R>
+void clover_blocks(const R **ddg, const typename C2<R>::T **dod, const R **idg, const typename C2<R>::T **iod);
+int clover_apply(int which, double mass, void *out, const void *in, int par);
+
+// dispatch helper for kernels templated on NF and on real/complex links
+#define HR_NF_DISPATCH(REAL, NF, CALL)                                                     \
+  do {                                                                                     \
+    if (!(REAL)) {                                                                         \
+      switch (NF) {                                                                        \
+        case 2: { constexpr int N_ = 2; constexpr bool R_ = false; CALL; } break;           \
+        case 3: { constexpr int N_ = 3; constexpr bool R_ = false; CALL; } break;           \
+        case 4: { constexpr int N_ = 4; constexpr bool R_ = false; CALL; } break;           \
+        case 5: { constexpr int N_ = 5; constexpr bool R_ = false; CALL; } break;           \
+        case 6: { constexpr int N_ = 6; constexpr bool R_ = false; CALL; } break;           \
+        case 10: { constexpr int N_ = 10; constexpr bool R_ = false; CALL; } break;         \
+        default: set_error("no kernel instantiated for complex NF=%d", (int)(NF)); return HRGPU_E_NF; \
+      }                                                                                    \
+    } else {                                                                               \
+      switch (NF) {                                                                        \
+        case 3: { constexpr int N_ = 3; constexpr bool R_ = true; CALL; } break;            \
+        case 8: { constexpr int N_ = 8; constexpr bool R_ = true; CALL; } break;            \
+        case 15: { constexpr int N_ = 15; constexpr bool R_ = true; CALL; } break;          \
+        default: set_error("no kernel instantiated for real NF=%d", (int)(NF)); return HRGPU_E_NF; \
+      }                                                                                    \
+    }                                                                                      \
+  } while (0)
+
+// dispatch over every NF of the lists above, complex data (clover blocks exist
+// as complex matrices for real representations too)
+#define HR_NFC_DISPATCH(NF, CALL)                                                          \
+  do {                                                                                     \
+    switch (NF) {                                                                          \
+      case 2: { constexpr int N_ = 2; CALL; } break;                                        \
+      case 3: { constexpr int N_ = 3; CALL; } break;                                        \
+      case 4: { constexpr int N_ = 4; CALL; } break;                                        \
+      case 5: { constexpr int N_ = 5; CALL; } break;                                        \
+      case 6: { constexpr int N_ = 6; CALL; } break;                                        \
+      case 8: { constexpr int N_ = 8; CALL; } break;                                        \
+      case 10: { constexpr int N_ = 10; CALL; } break;                                      \
+      case 15: { constexpr int N_ = 15; CALL; } break;                                      \
+      default: set_error("no kernel instantiated for NF=%d", (int)(NF)); return HRGPU_E_NF; \
+    }                                                                                      \
+  } while (0)
+
+// device index of the neighbour of (t,x,y,z) in direction mu (dir=+1/-1)
+__device__ __forceinline__ int nbr_index(const Geo &g, int t, int x, int y, int z, int mu, int dir) {
+  if (mu == 0) t = (t + dir + g.T) % g.T;
+  if (mu == 1) x = (x + dir + g.X) % g.X;
+  if (mu == 2) y = (y + dir + g.Y) % g.Y;
+  if (mu == 3) z = (z + dir + g.Z) % g.Z;
+  return ((t + x + y + z) & 1) * g.ld + coords_to_cb(g, t, x, y, z);
+}
+
+__device__ __forceinline__ void dev_coords(const Geo &g, int d, int &t, int &x, int &y, int &z) {
+  int p = d >= g.ld ? 1 : 0;
+  cb_to_coords(g, d - p * g.ld, p, t, x, y, z);
+}
+
+// small dense complex matrices in registers/local memory (row-major N x N)
+template <int N>
+struct CMat {
+  double2 c[N * N];
+};
+
+template <int N, bool REAL>
+__device__ __forceinline__ void mload(CMat<N> &m, const void *U, int mu, long d, long lplane) {
+  if (REAL) {
+    const double *u = (const double *)U + (long)mu * N * N * lplane + d;
+#pragma unroll (N <= 3 ? N * N : 1)
+    for (int k = 0; k < N * N; k++) m.c[k] = make_double2(__ldg(u + (long)k * lplane), 0.0);
+  } else {
+    const double2 *u = (const double2 *)U + (long)mu * N * N * lplane + d;
+#pragma unroll (N <= 3 ? N * N : 1)
+    for (int k = 0; k < N * N; k++) m.c[k] = __ldg(u + (long)k * lplane);
+  }
+}
+
+// C = op(A) op(B), with op = identity or dagger
+template <int N> struct SmallUnroll { static constexpr int v = N <= 3 ? N : 1; };
+
+template <int N, bool DA, bool DB>
+__device__ __forceinline__ void mmul(CMat<N> &C, const CMat<N> &A, const CMat<N> &B) {
+#pragma unroll (SmallUnroll<N>::v)
+  for (int i = 0; i < N; i++)
+#pragma unroll (SmallUnroll<N>::v)
+    for (int j = 0; j < N; j++) {
+      double2 s = make_double2(0.0, 0.0);
+#pragma unroll (SmallUnroll<N>::v)
+      for (int k = 0; k < N; k++) {
+        double2 a = DA ? make_double2(A.c[k * N + i].x, -A.c[k * N + i].y) : A.c[i * N + k];
+        double2 b = DB ? make_double2(B.c[j * N + k].x, -B.c[j * N + k].y) : B.c[k * N + j];
+        cmac(s, a, b);
+      }
+      C.c[i * N + j] = s;
+    }
+}
+
+template <int N>
+__device__ __forceinline__ void madd(CMat<N> &A, const CMat<N> &B) {
+#pragma unroll (SmallUnroll<N * N>::v)
+  for (int k = 0; k < N * N; k++) A.c[k] = cadd(A.c[k], B.c[k]);
+}
+
+}  // namespace hrgpu

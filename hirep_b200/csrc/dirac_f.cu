@@ -1,0 +1,6 @@
+// single-precision instantiation of the hopping kernels
+#include "hop_launch.cuh"
+
+namespace hrgpu {
+template int launch_hop<float>(int, HopArgs<float> &);
+}

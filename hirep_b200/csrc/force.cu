@@ -1,0 +1,387 @@
+// force.cu -- pseudofermion force on the device (LibHR/Update/force_fermion_core.c
+// and the clover derivative of LibHR/Update/clover_tools.c:208-310).
+//
+// The force is the adjoint of the hopping term: per link, the spin-projected
+// colour outer products of X and Y at x and x+mu (HiRep's _F_DIR0.._F_DIR3 and
+// _suNf_FMAT) times the link, projected onto the algebra with the generators of
+// the representation (a sparse table built at lattice set-up), scaled by
+// -residue*dt*C(R)/C(F).  One thread per (site, direction).
+#include "dirac.cuh"
+
+namespace hrgpu {
+
+static inline unsigned nb(long n, int t = 128) { return (unsigned)((n + t - 1) / t); }
+
+struct ProjTab {
+  const int *off, *k;
+  const double2 *c;
+  int dimg;
+};
+
+// h_A += coeff * Re sum_k c_Ak m_k, into force planes [mu][A][2ld]
+template <int N>
+__device__ __forceinline__ void project_add(const double2 (&m)[N * N], const ProjTab &P, double *f, long lp, int mu,
+                                            long d, double coeff) {
+  for (int A = 0; A < P.dimg; A++) {
+    double s = 0.0;
+    for (int q = P.off[A]; q < P.off[A + 1]; q++) {
+      double2 c = P.c[q], v = m[P.k[q]];
+      s += c.x * v.x - c.y * v.y;
+    }
+    f[((long)mu * P.dimg + A) * lp + d] += coeff * s;
+  }
+}
+
+// full-lattice spinor element (component c) at device site d
+__device__ __forceinline__ const double2 *sp_at(const double2 *f, long d, int c, int ld, int nf) {
+  int p = d >= ld ? 1 : 0;
+  return f + ((long)p * 4 * nf + c) * ld + (d - (long)p * ld);
+}
+
+// one _F_DIRmu(s1, chi1, chi2) accumulation: chi1 at x, chi2 at x+mu
+template <int N, bool REAL>
+__device__ __forceinline__ void f_dir(double2 (&s1)[N * N], const void *U, long lp, int mu, long dx, long dy,
+                                      const double2 *c1, const double2 *c2, int ld) {
+  double2 pt[N], pt2[N], p0[N], p1[N], p2[N], p3[N];
+  for (int i = 0; i < N; i++) {
+    double2 a0 = *sp_at(c2, dy, i, ld, N), a1 = *sp_at(c2, dy, N + i, ld, N);
+    double2 a2 = *sp_at(c2, dy, 2 * N + i, ld, N), a3 = *sp_at(c2, dy, 3 * N + i, ld, N);
+    double2 b0 = *sp_at(c1, dx, i, ld, N), b1 = *sp_at(c1, dx, N + i, ld, N);
+    double2 b2 = *sp_at(c1, dx, 2 * N + i, ld, N), b3 = *sp_at(c1, dx, 3 * N + i, ld, N);
+    if (mu == 0) { pt[i] = cadd(a0, a2); pt2[i] = cadd(a1, a3); p2[i] = csub(b0, b2); p3[i] = csub(b1, b3); }
+    if (mu == 1) { pt[i] = caddi(a0, a3); pt2[i] = caddi(a1, a2); p2[i] = csubi(b0, b3); p3[i] = csubi(b1, b2); }
+    if (mu == 2) { pt[i] = cadd(a0, a3); pt2[i] = csub(a1, a2); p2[i] = csub(b0, b3); p3[i] = cadd(b1, b2); }
+    if (mu == 3) { pt[i] = caddi(a0, a2); pt2[i] = csubi(a1, a3); p2[i] = csubi(b0, b2); p3[i] = caddi(b1, b3); }
+  }
+  for (int i = 0; i < N; i++) {
+    double2 u0 = make_double2(0, 0), u1 = make_double2(0, 0);
+    for (int j = 0; j < N; j++) {
+      long idx = ((long)mu * N * N + i * N + j) * lp + dx;
+      if (REAL) {
+        double u = ((const double *)U)[idx];
+        rmac(u0, u, pt[j]);
+        rmac(u1, u, pt2[j]);
+      } else {
+        double2 u = ((const double2 *)U)[idx];
+        cmac(u0, u, pt[j]);
+        cmac(u1, u, pt2[j]);
+      }
+    }
+    p0[i] = u0;
+    p1[i] = u1;
+  }
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < N; j++) {
+      // s1_ij += p0_i conj(p2_j) + p1_i conj(p3_j)   (real part only for real representations)
+      double2 &s = s1[i * N + j];
+      s.x += p0[i].x * p2[j].x + p0[i].y * p2[j].y + p1[i].x * p3[j].x + p1[i].y * p3[j].y;
+      if (!REAL) s.y += p0[i].y * p2[j].x - p0[i].x * p2[j].y + p1[i].y * p3[j].x - p1[i].x * p3[j].y;
+    }
+}
+
+// force_fermion_core hopping part (force_fermion_core.c:848-923)
+template <int N, bool REAL>
+__global__ void k_force_hop(double *fsum, const void *U, const double2 *X, const double2 *Y, Geo g, ProjTab P,
+                            double coeff) {
+  long d = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  int mu = blockIdx.y;
+  if (d >= 2L * g.ld) return;
+  int p = d >= g.ld ? 1 : 0;
+  if (d - p * g.ld >= g.VH) return;
+  int t, x, y, z;
+  dev_coords(g, (int)d, t, x, y, z);
+  long dy = nbr_index(g, t, x, y, z, mu, +1);
+  const long lp = 2L * g.ld;
+  double2 s1[N * N];
+  for (int k = 0; k < N * N; k++) s1[k] = make_double2(0, 0);
+  f_dir<N, REAL>(s1, U, lp, mu, d, dy, X, Y, g.ld);
+  f_dir<N, REAL>(s1, U, lp, mu, d, dy, Y, X, g.ld);
+  project_add<N>(s1, P, fsum, lp, mu, d, coeff);
+}
+
+// g5 sigma_{mu nu} on a spinor held as [4][N] (force_fermion_core.c:123-250)
+template <int N>
+__device__ __forceinline__ void g5_sigma(double2 (&s)[4][N], const double2 (&u)[4][N], int q) {
+  // q enumerates (0,1),(0,2),(1,2),(0,3),(1,3),(2,3) as cl_force does
+  const int srcs[6][4] = {{1, 0, 3, 2}, {1, 0, 3, 2}, {0, 1, 2, 3}, {0, 1, 2, 3}, {1, 0, 3, 2}, {1, 0, 3, 2}};
+  // factors (re, im)
+  const double fr[6][4] = {{0, 0, 0, 0}, {-1, 1, -1, 1}, {0, 0, 0, 0}, {0, 0, 0, 0}, {-1, 1, 1, -1}, {0, 0, 0, 0}};
+  const double fi[6][4] = {{-1, -1, -1, -1}, {0, 0, 0, 0}, {1, -1, -1, 1}, {-1, 1, -1, 1}, {0, 0, 0, 0}, {1, 1, -1, -1}};
+  for (int c = 0; c < 4; c++)
+    for (int i = 0; i < N; i++) {
+      double2 a = u[srcs[q][c]][i];
+      s[c][i] = make_double2(fr[q][c] * a.x - fi[q][c] * a.y, fr[q][c] * a.y + fi[q][c] * a.x);
+    }
+}
+
+// force_clover_fermion (force_fermion_core.c:384-454)
+template <int N, bool REAL>
+__global__ void k_force_clover_fermion(double2 *clf, const double2 *X, const double2 *Y, Geo g, double residue) {
+  long d = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  int q = blockIdx.y;
+  if (d >= 2L * g.ld) return;
+  int p = d >= g.ld ? 1 : 0;
+  if (d - p * g.ld >= g.VH) return;
+  double2 xs[4][N], ys[4][N], tl[4][N], tr[4][N];
+  for (int c = 0; c < 4; c++)
+    for (int i = 0; i < N; i++) {
+      xs[c][i] = *sp_at(X, d, c * N + i, g.ld, N);
+      ys[c][i] = *sp_at(Y, d, c * N + i, g.ld, N);
+    }
+  g5_sigma<N>(tr, xs, q);
+  g5_sigma<N>(tl, ys, q);
+  const long lp = 2L * g.ld;
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < N; j++) {
+      double2 s = make_double2(0, 0);
+      for (int k = 0; k < 4; k++) {
+        cmacc(s, xs[k][j], tl[k][i]);  // tl_i conj(X_j)
+        cmacc(s, ys[k][j], tr[k][i]);  // tr_i conj(Y_j)
+      }
+      if (REAL) s.y = 0.0;
+      double2 &o = clf[((long)q * N * N + i * N + j) * lp + d];
+      o.x += residue * s.x;
+      o.y += residue * s.y;
+    }
+}
+
+// force_clover_core (force_fermion_core.c:282-379): one thread per (site, mu)
+template <int N, bool REAL>
+__global__ void k_force_clover_core(double *fsum, const void *U, const double2 *clf, Geo g, ProjTab P, double coeff) {
+  long d = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  int mu = blockIdx.y;
+  if (d >= 2L * g.ld) return;
+  int p = d >= g.ld ? 1 : 0;
+  if (d - p * g.ld >= g.VH) return;
+  int t, x, y, z;
+  dev_coords(g, (int)d, t, x, y, z);
+  const long lp = 2L * g.ld;
+  for (int nu = 0; nu < 4; nu++) {
+    if (nu == mu) continue;
+    int c[4] = {t, x, y, z};
+    long o1 = nbr_index(g, t, x, y, z, mu, +1);
+    long o2 = nbr_index(g, t, x, y, z, nu, +1);
+    long o3 = nbr_index(g, t, x, y, z, nu, -1);
+    int cm[4] = {c[0], c[1], c[2], c[3]};
+    int L4[4] = {g.T, g.X, g.Y, g.Z};
+    cm[nu] = (cm[nu] - 1 + L4[nu]) % L4[nu];
+    long o4 = nbr_index(g, cm[0], cm[1], cm[2], cm[3], mu, +1);
+    int cp[4] = {c[0], c[1], c[2], c[3]};
+    cp[nu] = (cp[nu] + 1) % L4[nu];
+    long o5 = nbr_index(g, cp[0], cp[1], cp[2], cp[3], mu, +1);
+    int num, sign;
+    if (mu < nu) { num = nu * (nu - 1) / 2 + mu; sign = +1; }
+    else { num = mu * (mu - 1) / 2 + nu; sign = -1; }
+    CMat<N> W0, W1, W2, W3, W4, W5, W6, W7, W8, s1, s2, s3, fm, Z, a;
+    auto zload = [&](CMat<N> &m, long s) {
+      for (int k = 0; k < N * N; k++) m.c[k] = clf[((long)num * N * N + k) * lp + s];
+    };
+    // W0 = U(o3,mu)^+, W1 = U(o3,nu), W2 = U(o1,nu), W3 = U(o2,mu)^+, W4 = U(x,nu)^+, W5 = U(o4,nu)^+
+    for (int k = 0; k < N * N; k++) W0.c[k] = make_double2(0, 0);
+    {
+      CMat<N> tmpm;
+      mload<N, REAL>(tmpm, U, mu, o3, lp);
+      for (int i = 0; i < N; i++)
+        for (int j = 0; j < N; j++) W0.c[i * N + j] = make_double2(tmpm.c[j * N + i].x, -tmpm.c[j * N + i].y);
+      mload<N, REAL>(W1, U, nu, o3, lp);
+      mload<N, REAL>(W2, U, nu, o1, lp);
+      mload<N, REAL>(tmpm, U, mu, o2, lp);
+      for (int i = 0; i < N; i++)
+        for (int j = 0; j < N; j++) W3.c[i * N + j] = make_double2(tmpm.c[j * N + i].x, -tmpm.c[j * N + i].y);
+      mload<N, REAL>(tmpm, U, nu, d, lp);
+      for (int i = 0; i < N; i++)
+        for (int j = 0; j < N; j++) W4.c[i * N + j] = make_double2(tmpm.c[j * N + i].x, -tmpm.c[j * N + i].y);
+      mload<N, REAL>(tmpm, U, nu, o4, lp);
+      for (int i = 0; i < N; i++)
+        for (int j = 0; j < N; j++) W5.c[i * N + j] = make_double2(tmpm.c[j * N + i].x, -tmpm.c[j * N + i].y);
+    }
+    mmul<N, false, false>(W6, W0, W1);
+    mmul<N, false, false>(W7, W2, W3);
+    mmul<N, false, false>(s1, W5, W6);
+    mmul<N, false, false>(W8, W7, W4);
+    for (int k = 0; k < N * N; k++) W8.c[k] = csub(W8.c[k], s1.c[k]);
+    zload(Z, d);
+    mmul<N, false, false>(fm, W8, Z);
+    zload(Z, o1);
+    mmul<N, false, false>(s1, Z, W8);
+    madd(fm, s1);
+    zload(Z, o3);
+    mmul<N, false, false>(s1, W0, Z);
+    mmul<N, false, false>(s2, s1, W1);
+    zload(Z, o4);
+    mmul<N, false, false>(s3, Z, W6);
+    madd(s2, s3);
+    mmul<N, false, false>(s1, W5, s2);
+    for (int k = 0; k < N * N; k++) fm.c[k] = csub(fm.c[k], s1.c[k]);
+    zload(Z, o5);
+    mmul<N, false, false>(s1, W2, Z);
+    mmul<N, false, false>(s2, s1, W3);
+    zload(Z, o2);
+    mmul<N, false, false>(s3, W7, Z);
+    madd(s2, s3);
+    mmul<N, false, false>(s1, s2, W4);
+    madd(fm, s1);
+    mload<N, REAL>(a, U, mu, d, lp);
+    mmul<N, false, false>(s1, a, fm);
+    double2 m[N * N];
+    for (int k = 0; k < N * N; k++) m[k] = REAL ? make_double2(s1.c[k].x, 0.0) : s1.c[k];
+    project_add<N>(m, P, fsum, lp, mu, d, sign * coeff);
+  }
+}
+
+// _compute_clover_force (clover_tools.c:208-298) on odd sites from the packed inverse
+template <int N, bool REAL>
+__global__ void k_force_logdet(double2 *clf, const double *idg, const double2 *iod, Geo g, double coeff) {
+  int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cb >= g.VH) return;
+  const long lp = 2L * g.ld, d = (long)g.ld + cb;  // odd sites
+  const int n = 2 * N, no = N * (2 * N - 1);
+  auto Ael = [&](int b, int i, int j) -> double2 {  // coeff * (D^-1)_ij of block b
+    double2 v;
+    if (i == j) v = make_double2(idg[((long)b * n + i) * lp + d], 0.0);
+    else if (i > j) v = iod[((long)b * no + i * (i - 1) / 2 + j) * lp + d];
+    else {
+      double2 w = iod[((long)b * no + j * (j - 1) / 2 + i) * lp + d];
+      v = make_double2(w.x, -w.y);
+    }
+    return make_double2(coeff * v.x, coeff * v.y);
+  };
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < N; j++) {
+      int ij = i * N + j;
+      double2 a21 = Ael(0, i + N, j), a12c = Ael(0, j + N, i), a43 = Ael(1, i + N, j), a34c = Ael(1, j + N, i);
+      double2 a12 = make_double2(a12c.x, -a12c.y), a34 = make_double2(a34c.x, -a34c.y);
+      // the inverse is Hermitian, so conj(A[j][i]) = A[i][j] on both branches of the reference
+      double2 a11 = Ael(0, i, j), a22 = Ael(0, i + N, j + N), a33 = Ael(1, i, j), a44 = Ael(1, i + N, j + N);
+      double2 *f = clf + (long)ij * lp + d;
+      const long qs = (long)N * N * lp;
+      if (REAL) {
+        f[0 * qs].x += a12.y + a21.y - a34.y - a43.y;
+        f[1 * qs].x += a12.x - a21.x + a43.x - a34.x;
+        f[2 * qs].x += a22.y - a11.y + a44.y - a33.y;
+        f[3 * qs].x += a11.y - a22.y + a44.y - a33.y;
+        f[4 * qs].x += a12.x - a21.x + a34.x - a43.x;
+        f[5 * qs].x -= a12.y + a21.y + a34.y + a43.y;
+      } else {
+        double2 s;
+        // -= i (a12 + a21 - a34 - a43)
+        s = make_double2(a12.x + a21.x - a34.x - a43.x, a12.y + a21.y - a34.y - a43.y);
+        f[0 * qs].x += s.y; f[0 * qs].y -= s.x;
+        s = make_double2(a12.x - a21.x + a43.x - a34.x, a12.y - a21.y + a43.y - a34.y);
+        f[1 * qs].x += s.x; f[1 * qs].y += s.y;
+        s = make_double2(a22.x - a11.x + a44.x - a33.x, a22.y - a11.y + a44.y - a33.y);
+        f[2 * qs].x += s.y; f[2 * qs].y -= s.x;
+        s = make_double2(a11.x - a22.x + a44.x - a33.x, a11.y - a22.y + a44.y - a33.y);
+        f[3 * qs].x += s.y; f[3 * qs].y -= s.x;
+        s = make_double2(a12.x - a21.x + a34.x - a43.x, a12.y - a21.y + a34.y - a43.y);
+        f[4 * qs].x += s.x; f[4 * qs].y += s.y;
+        // += i (a12 + a21 + a34 + a43)
+        s = make_double2(a12.x + a21.x + a34.x + a43.x, a12.y + a21.y + a34.y + a43.y);
+        f[5 * qs].x -= s.y; f[5 * qs].y += s.x;
+      }
+    }
+}
+
+static ProjTab proj() {
+  ProjTab P;
+  P.off = L.d_proj_off;
+  P.k = L.d_proj_k;
+  P.c = L.d_proj_c;
+  P.dimg = L.dimg;
+  return P;
+}
+
+static int ensure_force() {
+  if (!L.force_sum) {
+    size_t b = sizeof(double) * 4 * L.dimg * 2 * L.ld;
+    HR_CUDA(cudaMalloc(&L.force_sum, b));
+    HR_CUDA(cudaMemsetAsync(L.force_sum, 0, b, L.stream));
+  }
+  return 0;
+}
+
+int links_out(void *host, const void *dev, int nel, int elem_bytes, int ndir);
+
+}  // namespace hrgpu
+
+using namespace hrgpu;
+
+extern "C" {
+
+int hrgpu_fermion_force_begin(void) {
+  HR_REQUIRE(L.ready, HRGPU_E_STATE, "fermion_force_begin: lattice not initialised");
+  if (int rc = ensure_force()) return rc;
+  HR_CUDA(cudaMemsetAsync(L.force_sum, 0, sizeof(double) * 4 * L.dimg * 2 * L.ld, L.stream));
+  if (L.clover && L.cl_force)
+    HR_CUDA(cudaMemsetAsync(L.cl_force, 0, sizeof(double2) * 6 * L.nf * L.nf * 2 * L.ld, L.stream));
+  return 0;
+}
+
+int hrgpu_force_fermion_core(void *Xs, void *Ys, int auto_fill_odd, double dt, double residue) {
+  if (int rc = check_gauge(HRGPU_DOUBLE)) return rc;
+  HR_REQUIRE(Xs && Ys && Xs != Ys, HRGPU_E_ARG, "force_fermion_core: bad fields");
+  if (int rc = ensure_force()) return rc;
+  const size_t half = (size_t)4 * L.nf * L.ld;
+  double2 *X = (double2 *)Xs, *Y = (double2 *)Ys;
+  if (auto_fill_odd) {
+    const double mass = static_mass();
+    if (L.clover) {
+      if (int rc = clover_prepare(mass, HRGPU_DOUBLE)) return rc;
+      const double *ddg, *idg;
+      const double2 *dod, *iod;
+      clover_blocks<double>(&ddg, &dod, &idg, &iod);
+      if (int rc = hop<double>(HRGPU_ODD, X + half, X, EP_CLOV_INV, -0.5, nullptr, 0.0, 0, nullptr, idg, iod)) return rc;
+      if (int rc = hop<double>(HRGPU_ODD, Y + half, Y, EP_CLOV_INV, -0.5, nullptr, 0.0, 0, nullptr, idg, iod)) return rc;
+    } else {
+      if (int rc = hop<double>(HRGPU_ODD, X + half, X, EP_AXPY, -0.5, nullptr, 0.0, 0, nullptr, nullptr, nullptr)) return rc;
+      if (int rc = hop<double>(HRGPU_ODD, Y + half, Y, EP_AXPY, -0.5, nullptr, 0.0, 0, nullptr, nullptr, nullptr)) return rc;
+    }
+  }
+  // UPDATE_EO sign (force_fermion_core.c:825)
+  const double coeff = -residue * dt * (L.repr_norm2 / L.fund_norm2);
+  Geo g = make_geo();
+  const long n = 2L * L.ld;
+  if (L.clover) {
+    HR_NF_DISPATCH(L.real, L.nf, (k_force_clover_fermion<N_, R_><<<dim3(nb(n), 6), 128, 0, L.stream>>>(L.cl_force, X, Y, g, residue)));
+    HR_LAUNCH_CHECK();
+  }
+  HR_NF_DISPATCH(L.real, L.nf, (k_force_hop<N_, R_><<<dim3(nb(n), 4), 128, 0, L.stream>>>(L.force_sum, L.U, X, Y, g, proj(), coeff)));
+  HR_LAUNCH_CHECK();
+  return 0;
+}
+
+int hrgpu_force_clover_logdet(double mass, double residue) {
+  HR_REQUIRE(L.ready && L.clover, HRGPU_E_STATE, "force_clover_logdet: no clover term");
+  if (int rc = clover_prepare(mass, HRGPU_DOUBLE)) return rc;
+  Geo g = make_geo();
+  HR_NF_DISPATCH(L.real, L.nf, (k_force_logdet<N_, R_><<<nb(L.VH), 128, 0, L.stream>>>(L.cl_force, L.cl_idg, L.cl_iod, g, residue)));
+  HR_LAUNCH_CHECK();
+  return 0;
+}
+
+int hrgpu_fermion_force_end(double dt, double *force_host) {
+  HR_REQUIRE(L.ready && L.force_sum, HRGPU_E_STATE, "fermion_force_end: no force accumulated");
+  HR_REQUIRE(force_host, HRGPU_E_ARG, "fermion_force_end: NULL force field");
+  if (L.clover) {
+    if (int rc = check_gauge(HRGPU_DOUBLE)) return rc;
+    const double coeff = dt * (L.repr_norm2 / L.fund_norm2) * (1. / 8.) * L.csw;
+    Geo g = make_geo();
+    const long n = 2L * L.ld;
+    HR_NF_DISPATCH(L.real, L.nf, (k_force_clover_core<N_, R_><<<dim3(nb(n, 64), 4), 64, 0, L.stream>>>(L.force_sum, L.U, L.cl_force, g, proj(), coeff)));
+    HR_LAUNCH_CHECK();
+  }
+  const size_t m = (size_t)L.V * 4 * L.dimg;
+  double *tmp = new double[m];
+  int rc = links_out(tmp, L.force_sum, L.dimg, 8, 4);
+  if (rc == 0)
+    for (size_t i = 0; i < m; i++) force_host[i] += tmp[i];
+  delete[] tmp;
+  return rc;
+}
+
+int hrgpu_force_sum_get(double *host) {
+  HR_REQUIRE(L.ready && L.force_sum, HRGPU_E_STATE, "force_sum_get: no force accumulated");
+  return links_out(host, L.force_sum, L.dimg, 8, 4);
+}
+
+}  // extern "C"

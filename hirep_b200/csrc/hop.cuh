@@ -1,0 +1,297 @@
+// hop.cuh -- the even-odd Wilson hopping kernel (HiRep's Dphi_, LibHR/Update/Dphi.c:193-374)
+// with fused epilogues for the preconditioned and clover operators.
+//
+// One thread per output site of one parity.  Per direction the thread loads the
+// neighbour spinor from structure-of-arrays planes (consecutive threads read
+// consecutive 16-byte complex numbers), spin-projects it to two NF-vectors,
+// multiplies by U or U^+ streamed element by element from the link planes, and
+// accumulates the four spin components of the result in registers.  Neighbours
+// are computed from the coordinates (no index tables are read).
+//
+// Epilogues (all written with the -1/2 of Dphi_ folded into `cacc`):
+//   EP_AXPY      out = cacc*acc + caux*aux          (Dphi, eopre second hop)
+//   EP_CLOV_INV  out = Hinv (cacc*acc)              (Cphi_eopre first hop: D_oo^-1 D_oe)
+//   EP_CLOV      out = cacc*acc + Hdiag*aux         (Cphi, Cphi_eopre second hop)
+// then optionally gamma_5, and optionally a per-block partial of |out|^2.
+#pragma once
+#include <type_traits>
+
+#include "hrgpu_internal.cuh"
+
+namespace hrgpu {
+
+enum { EP_AXPY = 0, EP_CLOV_INV = 1, EP_CLOV = 2 };
+constexpr int HOP_THREADS = 128;
+
+template <typename R>
+struct HopArgs {
+  const void *in;    // input parity field, planes [4NF][ld]
+  void *out;         // output parity field
+  const void *U;     // links [4][NF*NF][2ld]
+  const void *aux;   // field at the output sites (EP_AXPY, EP_CLOV)
+  const R *cdg;      // packed clover diag [2][2NF][2ld] (Hdiag or Hinv)
+  const typename C2<R>::T *cod;  // packed clover off-diagonal [2][NF(2NF-1)][2ld]
+  double *red;       // block partials of |out|^2 (or nullptr)
+  const int *stop;   // inverter state: when non-null and *stop != 0 the launch does nothing
+  R cacc, caux;
+  int outp;
+  int g5;
+  int nf;
+  Geo g;
+};
+
+template <bool REAL, typename R>
+struct LinkE {
+  typedef typename C2<R>::T T;
+};
+template <typename R>
+struct LinkE<true, R> {
+  typedef R T;
+};
+
+template <typename V> __device__ __forceinline__ V ld_c(const V *p) { return __ldg(p); }
+__device__ __forceinline__ double ld_c(const double *p) { return __ldg(p); }
+__device__ __forceinline__ float ld_c(const float *p) { return __ldg(p); }
+
+// chi = U h (DAG=false) or U^+ h (DAG=true); U element (i,j) at U[(i*nf+j)*plane + site]
+template <int NA> struct Unroll { static constexpr int v = NA <= 12 ? NA : 1; };
+
+template <int NA, bool DAG, typename V>
+__device__ __forceinline__ void link_mul(V *chi, const V *h, const V *U, long plane, long site, int nf) {
+#pragma unroll
+  for (int i = 0; i < NA; i++) {
+    if (i >= nf) break;
+    V a = cmk<V>(0.0, 0.0);
+#pragma unroll (Unroll<NA>::v)
+    for (int j = 0; j < NA; j++) {
+      if (j >= nf) break;
+      if (!DAG) {
+        V u = ld_c(U + (long)(i * nf + j) * plane + site);
+        cmac(a, u, h[j]);
+      } else {
+        V u = ld_c(U + (long)(j * nf + i) * plane + site);
+        cmacc(a, u, h[j]);
+      }
+    }
+    chi[i] = a;
+  }
+}
+
+template <int NA, bool DAG, typename V, typename R>
+__device__ __forceinline__ void link_mul(V *chi, const V *h, const R *U, long plane, long site, int nf) {
+#pragma unroll
+  for (int i = 0; i < NA; i++) {
+    if (i >= nf) break;
+    V a = cmk<V>(0.0, 0.0);
+#pragma unroll (Unroll<NA>::v)
+    for (int j = 0; j < NA; j++) {
+      if (j >= nf) break;
+      R u = DAG ? ld_c(U + (long)(j * nf + i) * plane + site) : ld_c(U + (long)(i * nf + j) * plane + site);
+      rmac(a, u, h[j]);
+    }
+    chi[i] = a;
+  }
+}
+
+// y = H x for one packed Hermitian 2NF x 2NF block (diag real, strict lower complex)
+template <int NA, typename V, typename R>
+__device__ __forceinline__ void herm_apply(V *y, const V *x, const R *dg, const V *od, long plane, long site, int nf) {
+  const int n = 2 * nf;
+#pragma unroll
+  for (int i = 0; i < 2 * NA; i++) {
+    if (i >= n) break;
+    R d = ld_c(dg + (long)i * plane + site);
+    y[i] = cscale(d, x[i]);
+  }
+#pragma unroll (Unroll<2 * NA>::v)
+  for (int i = 1; i < 2 * NA; i++) {
+    if (i >= n) break;
+#pragma unroll (Unroll<2 * NA>::v)
+    for (int j = 0; j < 2 * NA; j++) {
+      if (j >= i) break;
+      V l = ld_c(od + (long)(i * (i - 1) / 2 + j) * plane + site);
+      cmac(y[i], l, x[j]);   // y_i += L_ij x_j
+      cmacc(y[j], l, x[i]);  // y_j += conj(L_ij) x_i
+    }
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ void block_partial(double v, double *red) {
+  __shared__ double sh[HOP_THREADS / 32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) s += sh[k];
+    red[blockIdx.x] = s;
+  }
+}
+
+// clover epilogue on one chiral block: (ra, rb) are the spin pair of block b
+template <int NA, int EP, typename V, typename R>
+__device__ __forceinline__ void clover_epilogue(V (&ra)[NA], V (&rb)[NA], const HopArgs<R> &a, R ca, int cb, int b) {
+  const Geo &g = a.g;
+  const int nf = NA;
+  const long ld = g.ld, lp = 2L * g.ld, site = (long)a.outp * g.ld + cb;
+  const int n2 = 2 * nf, no = nf * (2 * nf - 1);
+  V xin[2 * NA], yout[2 * NA];
+  if (EP == EP_CLOV_INV) {
+#pragma unroll
+    for (int i = 0; i < NA; i++) {
+      xin[i] = cscale(ca, ra[i]);
+      xin[nf + i] = cscale(ca, rb[i]);
+    }
+  } else {
+    const V *aux = (const V *)a.aux + cb;
+#pragma unroll
+    for (int i = 0; i < NA; i++) {
+      xin[i] = ld_c(aux + (long)((2 * b) * nf + i) * ld);
+      xin[nf + i] = ld_c(aux + (long)((2 * b + 1) * nf + i) * ld);
+    }
+  }
+  herm_apply<NA>(yout, xin, a.cdg + (long)b * n2 * lp, a.cod + (long)b * no * lp, lp, site, nf);
+#pragma unroll
+  for (int i = 0; i < NA; i++) {
+    if (EP == EP_CLOV_INV) {
+      ra[i] = yout[i];
+      rb[i] = yout[nf + i];
+    } else {
+      ra[i] = cadd(cscale(ca, ra[i]), yout[i]);
+      rb[i] = cadd(cscale(ca, rb[i]), yout[nf + i]);
+    }
+  }
+}
+
+template <int NFT, bool REAL, typename R, int EP>
+__global__ void __launch_bounds__(HOP_THREADS) k_hop(HopArgs<R> a) {
+  typedef typename C2<R>::T V;
+  typedef typename LinkE<REAL, R>::T E;
+  constexpr int NA = NFT;
+  const int nf = NFT;
+  const Geo g = a.g;
+  if (a.stop && *a.stop) return;
+  const int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = cb < g.VH;
+  double nrm = 0.0;
+  if (active) {
+    const int outp = a.outp, inp = outp ^ 1;
+    int t, x, y, z;
+    cb_to_coords(g, cb, outp, t, x, y, z);
+    const long ld = g.ld, lplane = 2L * g.ld;
+    const V *in = (const V *)a.in;
+    const E *U = (const E *)a.U;
+    const long nf2 = (long)nf * nf;
+    V r0[NA], r1[NA], r2[NA], r3[NA], h0[NA], h1[NA], c0[NA], c1[NA];
+#pragma unroll
+    for (int i = 0; i < NA; i++) r0[i] = r1[i] = r2[i] = r3[i] = cmk<V>(0.0, 0.0);
+    const long so = (long)outp * ld + cb;  // this site in the link planes
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++) {
+      int tp = t, xp = x, yp = y, zp = z, tm = t, xm = x, ym = y, zm = z;
+      if (mu == 0) { tp = (t + 1 == g.T) ? 0 : t + 1; tm = (t == 0) ? g.T - 1 : t - 1; }
+      if (mu == 1) { xp = (x + 1 == g.X) ? 0 : x + 1; xm = (x == 0) ? g.X - 1 : x - 1; }
+      if (mu == 2) { yp = (y + 1 == g.Y) ? 0 : y + 1; ym = (y == 0) ? g.Y - 1 : y - 1; }
+      if (mu == 3) { zp = (z + 1 == g.Z) ? 0 : z + 1; zm = (z == 0) ? g.Z - 1 : z - 1; }
+      const int cup = coords_to_cb(g, tp, xp, yp, zp);
+      const int cdn = coords_to_cb(g, tm, xm, ym, zm);
+      const E *Umu = U + (long)mu * nf2 * lplane;
+      // ---- forward: (1 - gamma_mu) U(x,mu) psi(x+mu)
+      {
+        const V *s = in + cup;
+#pragma unroll
+        for (int i = 0; i < NA; i++) {
+          if (i >= nf) break;
+          V s0 = ld_c(s + (long)(0 * nf + i) * ld), s1 = ld_c(s + (long)(1 * nf + i) * ld);
+          V s2 = ld_c(s + (long)(2 * nf + i) * ld), s3 = ld_c(s + (long)(3 * nf + i) * ld);
+          if (mu == 0) { h0[i] = cadd(s0, s2); h1[i] = cadd(s1, s3); }
+          if (mu == 1) { h0[i] = caddi(s0, s3); h1[i] = caddi(s1, s2); }
+          if (mu == 2) { h0[i] = cadd(s0, s3); h1[i] = csub(s1, s2); }
+          if (mu == 3) { h0[i] = caddi(s0, s2); h1[i] = csubi(s1, s3); }
+        }
+        link_mul<NA, false>(c0, h0, Umu, lplane, so, nf);
+        link_mul<NA, false>(c1, h1, Umu, lplane, so, nf);
+#pragma unroll
+        for (int i = 0; i < NA; i++) {
+          if (i >= nf) break;
+          r0[i] = cadd(r0[i], c0[i]);
+          r1[i] = cadd(r1[i], c1[i]);
+          if (mu == 0) { r2[i] = cadd(r2[i], c0[i]); r3[i] = cadd(r3[i], c1[i]); }
+          if (mu == 1) { r3[i] = csubi(r3[i], c0[i]); r2[i] = csubi(r2[i], c1[i]); }
+          if (mu == 2) { r3[i] = cadd(r3[i], c0[i]); r2[i] = csub(r2[i], c1[i]); }
+          if (mu == 3) { r2[i] = csubi(r2[i], c0[i]); r3[i] = caddi(r3[i], c1[i]); }
+        }
+      }
+      // ---- backward: (1 + gamma_mu) U(x-mu,mu)^+ psi(x-mu)
+      {
+        const V *s = in + cdn;
+#pragma unroll
+        for (int i = 0; i < NA; i++) {
+          if (i >= nf) break;
+          V s0 = ld_c(s + (long)(0 * nf + i) * ld), s1 = ld_c(s + (long)(1 * nf + i) * ld);
+          V s2 = ld_c(s + (long)(2 * nf + i) * ld), s3 = ld_c(s + (long)(3 * nf + i) * ld);
+          if (mu == 0) { h0[i] = csub(s0, s2); h1[i] = csub(s1, s3); }
+          if (mu == 1) { h0[i] = csubi(s0, s3); h1[i] = csubi(s1, s2); }
+          if (mu == 2) { h0[i] = csub(s0, s3); h1[i] = cadd(s1, s2); }
+          if (mu == 3) { h0[i] = csubi(s0, s2); h1[i] = caddi(s1, s3); }
+        }
+        const long sn = (long)inp * ld + cdn;
+        link_mul<NA, true>(c0, h0, Umu, lplane, sn, nf);
+        link_mul<NA, true>(c1, h1, Umu, lplane, sn, nf);
+#pragma unroll
+        for (int i = 0; i < NA; i++) {
+          if (i >= nf) break;
+          r0[i] = cadd(r0[i], c0[i]);
+          r1[i] = cadd(r1[i], c1[i]);
+          if (mu == 0) { r2[i] = csub(r2[i], c0[i]); r3[i] = csub(r3[i], c1[i]); }
+          if (mu == 1) { r3[i] = caddi(r3[i], c0[i]); r2[i] = caddi(r2[i], c1[i]); }
+          if (mu == 2) { r3[i] = csub(r3[i], c0[i]); r2[i] = cadd(r2[i], c1[i]); }
+          if (mu == 3) { r2[i] = caddi(r2[i], c0[i]); r3[i] = csubi(r3[i], c1[i]); }
+        }
+      }
+    }
+    // ---- epilogue
+    V *out = (V *)a.out + cb;
+    const R ca = a.cacc;
+    if (EP == EP_AXPY) {
+      const V *aux = (const V *)a.aux + cb;
+      const R cx = a.caux;
+#pragma unroll
+      for (int i = 0; i < NA; i++) {
+        if (i >= nf) break;
+        V q0 = cscale(ca, r0[i]), q1 = cscale(ca, r1[i]), q2 = cscale(ca, r2[i]), q3 = cscale(ca, r3[i]);
+        if (aux != nullptr && cx != (R)0) {
+          rmac(q0, cx, ld_c(aux + (long)(0 * nf + i) * ld));
+          rmac(q1, cx, ld_c(aux + (long)(1 * nf + i) * ld));
+          rmac(q2, cx, ld_c(aux + (long)(2 * nf + i) * ld));
+          rmac(q3, cx, ld_c(aux + (long)(3 * nf + i) * ld));
+        }
+        r0[i] = q0; r1[i] = q1; r2[i] = q2; r3[i] = q3;
+      }
+    } else {
+      // clover blocks: block 0 acts on spin (0,1), block 1 on spin (2,3)
+      clover_epilogue<NA, EP>(r0, r1, a, ca, cb, 0);
+      clover_epilogue<NA, EP>(r2, r3, a, ca, cb, 1);
+    }
+    const R sg = a.g5 ? (R)-1 : (R)1;
+#pragma unroll
+    for (int i = 0; i < NA; i++) {
+      if (i >= nf) break;
+      V o2 = cscale(sg, r2[i]), o3 = cscale(sg, r3[i]);
+      out[(long)(0 * nf + i) * ld] = r0[i];
+      out[(long)(1 * nf + i) * ld] = r1[i];
+      out[(long)(2 * nf + i) * ld] = o2;
+      out[(long)(3 * nf + i) * ld] = o3;
+      if (a.red) {
+        nrm += (double)r0[i].x * r0[i].x + (double)r0[i].y * r0[i].y + (double)r1[i].x * r1[i].x +
+               (double)r1[i].y * r1[i].y + (double)o2.x * o2.x + (double)o2.y * o2.y + (double)o3.x * o3.x +
+               (double)o3.y * o3.y;
+      }
+    }
+  }
+  if (a.red) block_partial<R>(nrm, a.red);
+}
+
+}  // namespace hrgpu

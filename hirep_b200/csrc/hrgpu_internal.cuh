@@ -1,0 +1,176 @@
+// hrgpu_internal.cuh -- shared definitions of the B200 fermion library.
+//
+// Device data layout (HBM), chosen for coalesced FP64/FP32 streaming:
+//   site index     d = p * ld + cb, p = (t+x+y+z)&1, cb = lex >> 1,
+//                  lex = ((t*Z + z)*Y + y)*X + x    (x fastest, X even)
+//   spinor field   one parity: [4*NF complex components][ld] as double2/float2
+//                  full lattice: [2 parities][4*NF][ld]
+//   links          [4 dirs][NF*NF elements][2*ld] (double2/float2, or double/float
+//                  for real representations)
+//   clover blocks  two Hermitian 2NF x 2NF blocks per site, packed lower
+//                  triangle: diag [2][2NF][2*ld] real, off [2][NF(2NF-1)][2*ld] complex
+// HiRep's own (host) layout and site numbering are translated at the boundary by
+// a permutation table built from HiRep's ipt[] map.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <string>
+
+#include "../../include/hrgpu.h"
+
+namespace hrgpu {
+
+// ---------------------------------------------------------------------------
+// error handling: every CUDA call is checked; failures set the library error
+// string and make the entry point return a non-zero status.
+// ---------------------------------------------------------------------------
+void set_error(const char *fmt, ...);
+int fail_cuda(cudaError_t e, const char *what, const char *file, int line);
+
+#define HR_CUDA(call)                                                   \
+  do {                                                                  \
+    cudaError_t _e = (call);                                            \
+    if (_e != cudaSuccess) return hrgpu::fail_cuda(_e, #call, __FILE__, __LINE__); \
+  } while (0)
+
+#define HR_LAUNCH_CHECK() HR_CUDA(cudaGetLastError())
+
+#define HR_REQUIRE(cond, code, ...)      \
+  do {                                   \
+    if (!(cond)) {                       \
+      hrgpu::set_error(__VA_ARGS__);     \
+      return (code);                     \
+    }                                    \
+  } while (0)
+
+constexpr int MAXNF = 64;
+constexpr int RED_THREADS = 256;
+constexpr int RED_MAX_BLOCKS = 1184;  // 8 x 148 SMs
+
+struct Lattice {
+  bool ready = false;
+  int T = 0, X = 0, Y = 0, Z = 0;
+  long V = 0, VH = 0;
+  int ld = 0;  // plane stride of one parity (>= VH, multiple of 32)
+  int ng = 0, nf = 0, repr = 0, real = 0, dimg = 0;
+  // HiRep site index -> device site index (p*ld+cb); and inverse
+  int *d_h2d = nullptr, *d_d2h = nullptr;
+  int *h_h2d = nullptr;
+  // gauge fields
+  void *U = nullptr;      // represented links, double (double2 or double)
+  void *Uf = nullptr;     // represented links, float
+  double2 *Ug = nullptr;  // fundamental links [4][ng*ng][2*ld]
+  bool have_gauge = false, have_gauge_flt = false, have_fund = false;
+  // clover
+  bool clover = false;
+  double csw = 0.0;
+  double sigma = 0xF00F;          // mass term (4+m) the inverse was built for
+  double2 *cl_term = nullptr;     // A blocks s0..s3 [4][nf*nf][2*ld]
+  double *cl_dg = nullptr;        // (4+m)+A packed: diag [2][2nf][2*ld]
+  double2 *cl_od = nullptr;       //                 off  [2][nf(2nf-1)][2*ld]
+  double *cl_idg = nullptr;       // inverse, same packing
+  double2 *cl_iod = nullptr;
+  float *cl_dg_f = nullptr, *cl_idg_f = nullptr;
+  float2 *cl_od_f = nullptr, *cl_iod_f = nullptr;
+  double sigma_diag = 0xF00F;     // mass term the packed diag was built for
+  double sigma_flt = 0xF00F;
+  // force
+  double *force_sum = nullptr;    // [4][dimg][2*ld]
+  double2 *cl_force = nullptr;    // [6][nf*nf][2*ld]
+  // algebra projection tables (sparse): for each generator A, entries (k=i*nf+j, coeff)
+  int *d_proj_off = nullptr;      // [dimg+1]
+  int *d_proj_k = nullptr;
+  double2 *d_proj_c = nullptr;    // conj(R(iT_A))_k / C(R)
+  double repr_norm2 = 0.0, fund_norm2 = 0.5;
+  double *h_rT = nullptr;         // host copy of R(iT_A) as complex pairs [dimg][nf*nf][2]
+  double *h_gT = nullptr;         // host copy of T_A [dimg][ng*ng][2]
+  // scratch
+  double *partials = nullptr;     // reduction partials (npart doubles, results after them)
+  long npart = 0;
+  double *h_partials = nullptr;   // pinned host mirror of the final values
+  double *d_scalars = nullptr;    // CG scalars
+  const int *cur_stop = nullptr;  // set by the inverters while they drive the operator
+  cudaStream_t stream = 0;
+  // temporaries (lazily allocated, sized for one parity unless noted)
+  void *tmp_o = nullptr, *tmp_e = nullptr, *tmp_e2 = nullptr, *tmp_full = nullptr, *tmp_full2 = nullptr;
+  void *tmp_o_f = nullptr, *tmp_e_f = nullptr, *tmp_full_f = nullptr;
+  void *stage = nullptr;
+  size_t stage_bytes = 0;
+};
+
+extern Lattice L;
+
+inline size_t spinor_elems(int par) { return (size_t)(par == HRGPU_FULL ? 2 : 1) * 4 * L.nf * L.ld; }
+inline size_t spinor_bytes(int par, int prec) {
+  return spinor_elems(par) * (prec == HRGPU_DOUBLE ? sizeof(double2) : sizeof(float2));
+}
+
+int ensure_tmp(void **p, size_t bytes);
+int compute_clover_term_dev();
+void cg_release();
+int ensure_stage(size_t bytes);
+
+// ---------------------------------------------------------------------------
+// small complex helpers
+// ---------------------------------------------------------------------------
+template <typename R> struct C2;
+template <> struct C2<double> { typedef double2 T; };
+template <> struct C2<float> { typedef float2 T; };
+
+template <typename V> __device__ __forceinline__ V cmk(double a, double b);
+template <> __device__ __forceinline__ double2 cmk<double2>(double a, double b) { return make_double2(a, b); }
+template <> __device__ __forceinline__ float2 cmk<float2>(double a, double b) { return make_float2((float)a, (float)b); }
+
+template <typename V> __device__ __forceinline__ V cadd(V a, V b) { V r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }
+template <typename V> __device__ __forceinline__ V csub(V a, V b) { V r; r.x = a.x - b.x; r.y = a.y - b.y; return r; }
+// a + i b, a - i b
+template <typename V> __device__ __forceinline__ V caddi(V a, V b) { V r; r.x = a.x - b.y; r.y = a.y + b.x; return r; }
+template <typename V> __device__ __forceinline__ V csubi(V a, V b) { V r; r.x = a.x + b.y; r.y = a.y - b.x; return r; }
+// acc += u * s
+template <typename V> __device__ __forceinline__ void cmac(V &acc, V u, V s) {
+  acc.x = fma(u.x, s.x, acc.x); acc.x = fma(-u.y, s.y, acc.x);
+  acc.y = fma(u.x, s.y, acc.y); acc.y = fma(u.y, s.x, acc.y);
+}
+// acc += conj(u) * s
+template <typename V> __device__ __forceinline__ void cmacc(V &acc, V u, V s) {
+  acc.x = fma(u.x, s.x, acc.x); acc.x = fma(u.y, s.y, acc.x);
+  acc.y = fma(u.x, s.y, acc.y); acc.y = fma(-u.y, s.x, acc.y);
+}
+// acc += r * s (r real)
+template <typename V, typename R> __device__ __forceinline__ void rmac(V &acc, R r, V s) {
+  acc.x = fma(r, s.x, acc.x); acc.y = fma(r, s.y, acc.y);
+}
+template <typename V, typename R> __device__ __forceinline__ V cscale(R r, V a) { V o; o.x = r * a.x; o.y = r * a.y; return o; }
+
+// ---------------------------------------------------------------------------
+// lattice coordinates on the device
+// ---------------------------------------------------------------------------
+struct Geo {
+  int X, Y, Z, T;  // sizes
+  int Xh;          // X/2
+  int ld;
+  int VH;
+};
+
+__device__ __forceinline__ void cb_to_coords(const Geo &g, int cb, int p, int &t, int &x, int &y, int &z) {
+  int xh = cb % g.Xh;
+  int row = cb / g.Xh;
+  y = row % g.Y;
+  row /= g.Y;
+  z = row % g.Z;
+  t = row / g.Z;
+  x = 2 * xh + ((p + t + y + z) & 1);
+}
+
+__device__ __forceinline__ int coords_to_cb(const Geo &g, int t, int x, int y, int z) {
+  return (((t * g.Z + z) * g.Y + y) * g.X + x) >> 1;
+}
+
+Geo make_geo();
+
+// reductions: block partial sums written to L.partials, folded on the device
+int finish_reduction(int nblocks, int nvals, double *host_out);
+
+}  // namespace hrgpu

@@ -1,0 +1,275 @@
+"""Python host mirror of the B200 fermion library (libhrgpu.so, C ABI in include/hrgpu.h).
+
+The method names follow HiRep's C API (LibHR/Update/Dphi.c, D_update.c,
+LibHR/Inverters/linear_algebra.c, cg_mshift*.c, LibHR/Update/force_fermion_core.c),
+so host code and tests read like HiRep's own.  Device memory comes from
+PyTorch (plumbing only); every computation runs in libhrgpu.so.  There is no
+CPU fallback: if the library is missing the import fails.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhrgpu.so")
+
+EVEN, ODD, FULL = 0, 1, 2
+DOUBLE, FLOAT = 0, 1
+FUND, ADJ, SYM, ASYM = 0, 1, 2, 3
+OP_G5DPHI_SQ, OP_G5DPHI_EOPRE_SQ, OP_G5CPHI_EOPRE_SQ, OP_G5CPHI_SQ = 0, 1, 2, 3
+E_NOCONV = 5
+
+_lib = None
+
+
+class HRGPUError(RuntimeError):
+    pass
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise HRGPUError("libhrgpu.so is not built (run __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        L.hrgpu_last_error.restype = ctypes.c_char_p
+        L.hrgpu_spinor_bytes.restype = ctypes.c_size_t
+        L.hrgpu_getMVM.restype = ctypes.c_ulong
+        L.hrgpu_get_dirac_mass.restype = ctypes.c_double
+        _lib = L
+    return _lib
+
+
+def _check(rc, what):
+    if rc != 0:
+        msg = lib().hrgpu_last_error().decode()
+        raise HRGPUError(f"{what}: status {rc}: {msg}")
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+D = ctypes.c_double
+
+
+def geometry(T, X, Y, Z):
+    """HiRep's serial site maps (ipt, iup, idn) built by the library (no GPU needed)."""
+    V = T * X * Y * Z
+    ipt = np.empty(V, np.int32)
+    iup = np.empty(4 * V, np.int32)
+    idn = np.empty(4 * V, np.int32)
+    _check(lib().hrgpu_geometry(T, X, Y, Z, _ptr(ipt), _ptr(iup), _ptr(idn)), "geometry")
+    return ipt, iup, idn
+
+
+class Field:
+    """A device spinor field in the library layout (parity, precision)."""
+
+    def __init__(self, lat, par, prec=DOUBLE):
+        import torch
+
+        self.lat, self.par, self.prec = lat, par, prec
+        self.nbytes = lib().hrgpu_spinor_bytes(par, prec)
+        self.buf = torch.zeros(self.nbytes, dtype=torch.uint8, device="cuda")
+        self.ptr = ctypes.c_void_p(self.buf.data_ptr())
+
+    def upload(self, host):
+        dt = np.complex128 if self.prec == DOUBLE else np.complex64
+        host = np.ascontiguousarray(host, dt)
+        assert host.shape == (self.lat.nsites(self.par), 4, self.lat.nf), host.shape
+        _check(lib().hrgpu_spinor_upload(self.ptr, _ptr(host), self.par, self.prec), "spinor_upload")
+        return self
+
+    def download(self):
+        dt = np.complex128 if self.prec == DOUBLE else np.complex64
+        out = np.empty((self.lat.nsites(self.par), 4, self.lat.nf), dt)
+        _check(lib().hrgpu_spinor_download(_ptr(out), self.ptr, self.par, self.prec), "spinor_download")
+        return out
+
+
+class Lattice:
+    """One lattice on one GPU: geometry, gauge field, clover term, force accumulator."""
+
+    def __init__(self, T, X, Y, Z, ng, repr_, ipt=None, device=0):
+        import torch
+
+        self.L = lib()
+        if ipt is None:
+            ipt = geometry(T, X, Y, Z)[0]
+        _check(self.L.hrgpu_init(device), "init")
+        torch.cuda.set_device(device)
+        _check(self.L.hrgpu_set_stream(ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)), "set_stream")
+        ipt = np.ascontiguousarray(ipt, np.int32)
+        _check(self.L.hrgpu_lattice_init(T, X, Y, Z, ng, repr_, _ptr(ipt)), "lattice_init")
+        self.dims = (T, X, Y, Z)
+        self.V = T * X * Y * Z
+        self.VH = self.V // 2
+        self.ng, self.repr = ng, repr_
+        self.nf = self.L.hrgpu_nf()
+        self.real = repr_ == ADJ
+        self.dimg = ng * ng - 1
+
+    def nsites(self, par):
+        return self.V if par == FULL else self.VH
+
+    def field(self, par, prec=DOUBLE, host=None):
+        f = Field(self, par, prec)
+        if host is not None:
+            f.upload(host)
+        return f
+
+    def sync(self):
+        _check(self.L.hrgpu_synchronize(), "synchronize")
+
+    # gauge ---------------------------------------------------------------
+    def set_gauge_f(self, uf):
+        dt = np.float64 if self.real else np.complex128
+        uf = np.ascontiguousarray(uf, dt)
+        _check(self.L.hrgpu_gauge_set_f(_ptr(uf)), "gauge_set_f")
+
+    def set_gauge(self, u):
+        u = np.ascontiguousarray(u, np.complex128)
+        _check(self.L.hrgpu_gauge_set(_ptr(u)), "gauge_set")
+
+    def represent_gauge_field(self, bc_t_antiperiodic=True):
+        _check(self.L.hrgpu_represent_gauge_field(int(bool(bc_t_antiperiodic))), "represent_gauge_field")
+
+    def gauge_f(self):
+        dt = np.float64 if self.real else np.complex128
+        uf = np.empty((self.V, 4, self.nf, self.nf), dt)
+        _check(self.L.hrgpu_gauge_get_f(_ptr(uf)), "gauge_get_f")
+        return uf
+
+    # Dirac operator --------------------------------------------------------
+    def Dphi_(self, out, inp):
+        _check(self.L.hrgpu_Dphi_(out.ptr, out.par, inp.ptr), "Dphi_")
+
+    def Dphi_flt_(self, out, inp):
+        _check(self.L.hrgpu_Dphi_flt_(out.ptr, out.par, inp.ptr), "Dphi_flt_")
+
+    def _m(self, name, m, out, inp):
+        _check(getattr(self.L, "hrgpu_" + name)(D(m), out.ptr, inp.ptr), name)
+
+    def Dphi(self, m, out, inp): self._m("Dphi", m, out, inp)
+    def g5Dphi(self, m, out, inp): self._m("g5Dphi", m, out, inp)
+    def g5Dphi_sq(self, m, out, inp): self._m("g5Dphi_sq", m, out, inp)
+    def Dphi_eopre(self, m, out, inp): self._m("Dphi_eopre", m, out, inp)
+    def Dphi_oepre(self, m, out, inp): self._m("Dphi_oepre", m, out, inp)
+    def g5Dphi_eopre(self, m, out, inp): self._m("g5Dphi_eopre", m, out, inp)
+    def g5Dphi_eopre_sq(self, m, out, inp): self._m("g5Dphi_eopre_sq", m, out, inp)
+    def Dphi_flt(self, m, out, inp): self._m("Dphi_flt", m, out, inp)
+    def g5Dphi_flt(self, m, out, inp): self._m("g5Dphi_flt", m, out, inp)
+    def g5Dphi_sq_flt(self, m, out, inp): self._m("g5Dphi_sq_flt", m, out, inp)
+    def Dphi_eopre_flt(self, m, out, inp): self._m("Dphi_eopre_flt", m, out, inp)
+    def g5Dphi_eopre_flt(self, m, out, inp): self._m("g5Dphi_eopre_flt", m, out, inp)
+    def g5Dphi_eopre_sq_flt(self, m, out, inp): self._m("g5Dphi_eopre_sq_flt", m, out, inp)
+
+    def getMVM(self):
+        return self.L.hrgpu_getMVM()
+
+    def set_dirac_mass(self, m):
+        _check(self.L.hrgpu_set_dirac_mass(D(m)), "set_dirac_mass")
+
+    def H2(self, out, inp): _check(self.L.hrgpu_H2(out.ptr, inp.ptr), "H2")
+    def H(self, out, inp): _check(self.L.hrgpu_H(out.ptr, inp.ptr), "H")
+    def D(self, out, inp): _check(self.L.hrgpu_D(out.ptr, inp.ptr), "D")
+
+    # clover --------------------------------------------------------------
+    def clover_init(self, csw):
+        _check(self.L.hrgpu_clover_init(D(csw)), "clover_init")
+
+    def compute_clover_term(self):
+        _check(self.L.hrgpu_compute_clover_term(), "compute_clover_term")
+
+    def clover_term(self):
+        cl = np.empty((self.V, 4, self.nf, self.nf), np.complex128)
+        _check(self.L.hrgpu_clover_term_get(_ptr(cl)), "clover_term_get")
+        return cl
+
+    def Cphi(self, m, out, inp): self._m("Cphi", m, out, inp)
+    def g5Cphi(self, m, out, inp): self._m("g5Cphi", m, out, inp)
+    def g5Cphi_sq(self, m, out, inp): self._m("g5Cphi_sq", m, out, inp)
+    def Cphi_eopre(self, m, out, inp): self._m("Cphi_eopre", m, out, inp)
+    def g5Cphi_eopre(self, m, out, inp): self._m("g5Cphi_eopre", m, out, inp)
+    def g5Cphi_eopre_sq(self, m, out, inp): self._m("g5Cphi_eopre_sq", m, out, inp)
+    def g5Cphi_eopre_flt(self, m, out, inp): self._m("g5Cphi_eopre_flt", m, out, inp)
+    def g5Cphi_eopre_sq_flt(self, m, out, inp): self._m("g5Cphi_eopre_sq_flt", m, out, inp)
+
+    def Cphi_diag(self, m, out, inp):
+        _check(self.L.hrgpu_Cphi_diag(D(m), out.ptr, inp.ptr, out.par), "Cphi_diag")
+
+    def Cphi_diag_inv(self, m, out, inp):
+        _check(self.L.hrgpu_Cphi_diag_inv(D(m), out.ptr, inp.ptr, out.par), "Cphi_diag_inv")
+
+    # linear algebra --------------------------------------------------------
+    def la(self, name, *args):
+        """spinor_field_<name>_f / _f_flt: args as in HiRep; fields are Field objects."""
+        fields = [a for a in args if isinstance(a, Field)]
+        par, prec = fields[0].par, fields[0].prec
+        cargs = []
+        for a in args:
+            if isinstance(a, Field):
+                cargs.append(a.ptr)
+            elif isinstance(a, complex):
+                cargs += [D(a.real), D(a.imag)]
+            else:
+                cargs.append(D(a))
+        _check(getattr(self.L, "hrgpu_spinor_field_" + name)(par, prec, *cargs), "spinor_field_" + name)
+
+    def la_red(self, name, *fields, n=1):
+        res = (ctypes.c_double * 2)()
+        _check(getattr(self.L, "hrgpu_spinor_field_" + name)(fields[0].par, fields[0].prec,
+                                                              *[f.ptr for f in fields], res), name)
+        return res[0] if n == 1 else complex(res[0], res[1])
+
+    def sqnorm(self, f): return self.la_red("sqnorm", f)
+    def prod_re(self, a, b): return self.la_red("prod_re", a, b)
+    def prod_im(self, a, b): return self.la_red("prod_im", a, b)
+    def prod(self, a, b): return self.la_red("prod", a, b, n=2)
+    def g5_prod_re(self, a, b): return self.la_red("g5_prod_re", a, b)
+    def g5_prod_im(self, a, b): return self.la_red("g5_prod_im", a, b)
+
+    def assign_sd2s(self, out, inp):
+        _check(self.L.hrgpu_assign_sd2s(out.ptr, inp.ptr, inp.par), "assign_sd2s")
+
+    def assign_s2sd(self, out, inp):
+        _check(self.L.hrgpu_assign_s2sd(out.ptr, inp.ptr, inp.par), "assign_s2sd")
+
+    # inverters -------------------------------------------------------------
+    def cg_mshift(self, op, mass, shifts, err2, inp, outs, max_iter=0, flt=False):
+        n = len(shifts)
+        sh = np.ascontiguousarray(shifts, np.float64)
+        arr = (ctypes.c_void_p * n)(*[o.ptr.value for o in outs])
+        it = ctypes.c_int(0)
+        fn = self.L.hrgpu_cg_mshift_flt if flt else self.L.hrgpu_cg_mshift
+        rc = fn(op, D(mass), n, _ptr(sh), D(err2), max_iter, inp.ptr, arr, ctypes.byref(it))
+        if rc == E_NOCONV:
+            return it.value, False
+        _check(rc, "cg_mshift_flt" if flt else "cg_mshift")
+        return it.value, True
+
+    # force -------------------------------------------------------------------
+    def fermion_force_begin(self):
+        _check(self.L.hrgpu_fermion_force_begin(), "fermion_force_begin")
+
+    def force_fermion_core(self, Xs, Ys, auto_fill_odd, dt, residue):
+        _check(self.L.hrgpu_force_fermion_core(Xs.ptr, Ys.ptr, int(auto_fill_odd), D(dt), D(residue)),
+               "force_fermion_core")
+
+    def force_clover_logdet(self, mass, residue):
+        _check(self.L.hrgpu_force_clover_logdet(D(mass), D(residue)), "force_clover_logdet")
+
+    def fermion_force_end(self, dt, force):
+        force = np.ascontiguousarray(force, np.float64).copy()
+        _check(self.L.hrgpu_fermion_force_end(D(dt), _ptr(force)), "fermion_force_end")
+        return force
+
+    def force_sum(self):
+        f = np.empty((self.V, 4, self.dimg), np.float64)
+        _check(self.L.hrgpu_force_sum_get(_ptr(f)), "force_sum_get")
+        return f
+
+    def finalize(self):
+        _check(self.L.hrgpu_finalize(), "finalize")

@@ -1,0 +1,215 @@
+/*
+ * hrgpu.h -- C ABI of the B200 (sm_100a) fermion hot path for HiRep.
+ *
+ * Plain C, plain pointers and sizes.  One process drives one GPU; the library
+ * keeps HiRep's "global state" model (one lattice, one gauge field, one clover
+ * term, one force accumulator), like LibHR does through Include/global.h.
+ *
+ * Fields passed to the operators are DEVICE pointers in the library's device
+ * layout (structure-of-arrays, checkerboarded; see hrgpu_spinor_bytes).  Host
+ * fields in HiRep's own layout (Include/spinor_field.h:37-56, site order from
+ * LibHR/Geometry/geometry_mpi_eo.c) cross the boundary through
+ * hrgpu_spinor_upload / hrgpu_spinor_download, which translate the site order
+ * and the layout exactly.
+ *
+ * Every entry point returns 0 on success and a non-zero HRGPU_E* code on
+ * failure; hrgpu_last_error() gives the message.  (HiRep's own convention is
+ * error() -> exit, LibHR/Error/error.c:21-37; the drop-in layer maps a non-zero
+ * status onto that.)
+ *
+ * Each declaration names the reference interface it replaces (file:line in
+ * sofiemartins/HiRep).
+ */
+#ifndef HRGPU_H
+#define HRGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* parities: HiRep's glat_even / glat_odd / glattice (Include/global.h:105-107) */
+enum { HRGPU_EVEN = 0, HRGPU_ODD = 1, HRGPU_FULL = 2 };
+/* precisions: spinor_field / spinor_field_flt (Include/spinor_field.h:50-51) */
+enum { HRGPU_DOUBLE = 0, HRGPU_FLOAT = 1 };
+/* representations: REPR_FUNDAMENTAL / _ADJOINT / _SYMMETRIC / _ANTISYMMETRIC (Make/MkFlags) */
+enum { HRGPU_FUND = 0, HRGPU_ADJ = 1, HRGPU_SYM = 2, HRGPU_ASYM = 3 };
+/* operators for the inverters: the spinor_operator argument of cg_mshift (Include/inverters.h:14) */
+enum {
+  HRGPU_OP_G5DPHI_SQ = 0,       /* g5Dphi_sq(mass)        Dphi.c:1001-1019, full lattice   */
+  HRGPU_OP_G5DPHI_EOPRE_SQ = 1, /* g5Dphi_eopre_sq(mass)  Dphi.c:988-998, even sites       */
+  HRGPU_OP_G5CPHI_EOPRE_SQ = 2, /* g5Cphi_eopre_sq(mass)  Dphi.c:1263-1272, even sites     */
+  HRGPU_OP_G5CPHI_SQ = 3        /* g5Cphi_sq(mass)        Dphi.c:1226-1235, full lattice   */
+};
+/* status codes */
+enum {
+  HRGPU_OK = 0,
+  HRGPU_E_CUDA = 1,      /* a CUDA call failed                          */
+  HRGPU_E_ARG = 2,       /* invalid argument                            */
+  HRGPU_E_STATE = 3,     /* called before the state it needs was set    */
+  HRGPU_E_NF = 4,        /* no kernel instantiated for this NF          */
+  HRGPU_E_NOCONV = 5     /* inverter stopped at max_iter (not fatal)    */
+};
+
+/* ---------------------------------------------------------------- setup -- */
+/* process/device setup: replaces the device part of setup_process (LibHR/Geometry/process_init.c:56-146) */
+int hrgpu_init(int device);
+/* lattice: geometry_init (LibHR/Geometry/geometry_init.c:243-338) for one GPU.
+ * ipt is HiRep's site map ipt[((t*X+x)*Y+y)*Z+z] (Include/global.h:96,103) and is
+ * imported bit-exactly; ng/repr fix NG, NF and the representation (Make/MkFlags:1-75). */
+int hrgpu_lattice_init(int T, int X, int Y, int Z, int ng, int repr, const int *ipt);
+/* HiRep's serial site numbering (LibHR/Geometry/geometry_mpi_eo.c:1919-1953 with
+ * NP_T=NP_X=NP_Y=NP_Z=1): fills ipt[V] and, when non-NULL, iup[4V] and idn[4V]
+ * exactly as Include/global.h:96-100 holds them.  Host-only, no GPU needed. */
+int hrgpu_geometry(int T, int X, int Y, int Z, int *ipt, int *iup, int *idn);
+/* frees every device buffer (the atexit frees of Dphi.c:45-73, field_alloc.c) */
+int hrgpu_finalize(void);
+const char *hrgpu_last_error(void);
+int hrgpu_nf(void);
+/* bytes of one device spinor field of the given parity and precision */
+size_t hrgpu_spinor_bytes(int par, int prec);
+/* all work is issued on this stream (default: the library's own stream) */
+int hrgpu_set_stream(void *cuda_stream);
+int hrgpu_synchronize(void);
+
+/* --------------------------------------------------------- gauge fields -- */
+/* u_gauge upload (Include/global.h:143, HiRep layout [V][4][NG*NG] complex) */
+int hrgpu_gauge_set(const double *u_host);
+/* represent_gauge_field (LibHR/Update/representation.c:391-468) on the device, then
+ * the antiperiodic-T link sign (LibHR/Utils/boundary_conditions.c:321-341) and,
+ * with a clover term, compute_clover_term; also refreshes the float copy (assign_ud2u_f) */
+int hrgpu_represent_gauge_field(int bc_t_antiperiodic);
+/* u_gauge_f upload: the represented field as HiRep holds it ([V][4][NF*NF], complex,
+ * or real for the adjoint representation) */
+int hrgpu_gauge_set_f(const void *uf_host);
+int hrgpu_gauge_get_f(void *uf_host);
+/* assign_ud2u_f (LibHR/Utils/single_double_utils.c:70-87) */
+int hrgpu_assign_ud2u_f(void);
+
+/* ------------------------------------------------------- spinor fields -- */
+/* host (HiRep layout, HiRep site order) <-> device layout; prec selects
+ * suNf_spinor (double) or suNf_spinor_flt (float) */
+int hrgpu_spinor_upload(void *dev, const void *host, int par, int prec);
+int hrgpu_spinor_download(void *host, const void *dev, int par, int prec);
+/* assign_sd2s / assign_s2sd (LibHR/Utils/single_double_utils.c:89-115) */
+int hrgpu_assign_sd2s(void *out_flt, const void *in_dbl, int par);
+int hrgpu_assign_s2sd(void *out_dbl, const void *in_flt, int par);
+
+/* ------------------------------------------------------ Dirac operator -- */
+/* Dphi_ (LibHR/Update/Dphi.c:193-374): out_par EVEN/ODD reads the other parity,
+ * FULL reads a full field.  Hopping term with the -1/2 included. */
+int hrgpu_Dphi_(void *out, int out_par, const void *in);
+int hrgpu_Dphi(double m0, void *out, const void *in);             /* Dphi.c:703-783   */
+int hrgpu_g5Dphi(double m0, void *out, const void *in);           /* Dphi.c:785-867   */
+int hrgpu_g5Dphi_sq(double m0, void *out, const void *in);        /* Dphi.c:1001-1019 */
+int hrgpu_Dphi_eopre(double m0, void *out, const void *in);       /* Dphi.c:874-907   */
+int hrgpu_Dphi_oepre(double m0, void *out, const void *in);       /* Dphi.c:914-948   */
+int hrgpu_g5Dphi_eopre(double m0, void *out, const void *in);     /* Dphi.c:950-985   */
+int hrgpu_g5Dphi_eopre_sq(double m0, void *out, const void *in);  /* Dphi.c:988-998   */
+/* single precision: LibHR/Update/Dphi_flt.c:162-593 */
+int hrgpu_Dphi_flt_(void *out, int out_par, const void *in);
+int hrgpu_Dphi_flt(double m0, void *out, const void *in);
+int hrgpu_g5Dphi_flt(double m0, void *out, const void *in);
+int hrgpu_g5Dphi_sq_flt(double m0, void *out, const void *in);
+int hrgpu_Dphi_eopre_flt(double m0, void *out, const void *in);
+int hrgpu_g5Dphi_eopre_flt(double m0, void *out, const void *in);
+int hrgpu_g5Dphi_eopre_sq_flt(double m0, void *out, const void *in);
+/* getMVM (Dphi.c:105-113): hopping applications / 2 since the last call */
+unsigned long hrgpu_getMVM(void);
+
+/* set_dirac_mass / get_dirac_mass and the global-mass operators H2, H, D
+ * (LibHR/Update/D_update.c:12-95, UPDATE_EO build; clover forms when a clover
+ * term is set) */
+int hrgpu_set_dirac_mass(double mass);
+double hrgpu_get_dirac_mass(void);
+int hrgpu_H2(void *out, const void *in);
+int hrgpu_H(void *out, const void *in);
+int hrgpu_D(void *out, const void *in);
+
+/* ---------------------------------------------------------------- clover -- */
+int hrgpu_clover_init(double csw);                  /* clover_init, clover_tools.c:360-373        */
+int hrgpu_compute_clover_term(void);                /* compute_clover_term, clover_tools.c:333-341 */
+int hrgpu_compute_ldl_decomp(double sigma);         /* compute_ldl_decomp, clover_tools.c:343-358  */
+int hrgpu_clover_term_get(void *cl_host);           /* cl_term in HiRep layout [V][4][NF*NF] complex */
+int hrgpu_Cphi(double mass, void *out, const void *in);            /* Dphi.c:1215-1221 */
+int hrgpu_g5Cphi(double mass, void *out, const void *in);          /* Dphi.c:1223-1227 */
+int hrgpu_g5Cphi_sq(double mass, void *out, const void *in);       /* Dphi.c:1229-1238 */
+int hrgpu_Cphi_eopre(double mass, void *out, const void *in);      /* Dphi.c:1240-1255 */
+int hrgpu_g5Cphi_eopre(double mass, void *out, const void *in);    /* Dphi.c:1257-1261 */
+int hrgpu_g5Cphi_eopre_sq(double mass, void *out, const void *in); /* Dphi.c:1263-1272 */
+int hrgpu_Cphi_diag(double mass, void *out, const void *in, int par);     /* Dphi.c:1274-1280 */
+int hrgpu_Cphi_diag_inv(double mass, void *out, const void *in, int par); /* Dphi.c:1282-1288 */
+/* float clover operator for the mixed-precision solver (no float clover in the reference) */
+int hrgpu_g5Cphi_eopre_flt(double mass, void *out, const void *in);
+int hrgpu_g5Cphi_eopre_sq_flt(double mass, void *out, const void *in);
+
+/* -------------------------------------------------------- linear algebra -- */
+/* LibHR/Inverters/TMPL/linear_algebra.c.sdtmpl (declared in
+ * Include/TMPL/linear_algebra.h.sdtmpl:6-95), instantiated for double (_f) and
+ * float (_f_flt) by LibHR/Inverters/linear_algebra.c:20-59.  par gives the
+ * geometry of the fields; prec = HRGPU_DOUBLE or HRGPU_FLOAT.  Reductions
+ * accumulate in double in a fixed order (deterministic) and return on the host. */
+int hrgpu_spinor_field_prod_re(int par, int prec, const void *s1, const void *s2, double *res);
+int hrgpu_spinor_field_prod_im(int par, int prec, const void *s1, const void *s2, double *res);
+int hrgpu_spinor_field_prod(int par, int prec, const void *s1, const void *s2, double *res_re_im);
+int hrgpu_spinor_field_g5_prod_re(int par, int prec, const void *s1, const void *s2, double *res);
+int hrgpu_spinor_field_g5_prod_im(int par, int prec, const void *s1, const void *s2, double *res);
+int hrgpu_spinor_field_sqnorm(int par, int prec, const void *s1, double *res);
+int hrgpu_spinor_field_mul_add_assign(int par, int prec, void *s1, double r, const void *s2);
+int hrgpu_spinor_field_mulc_add_assign(int par, int prec, void *s1, double c_re, double c_im, const void *s2);
+int hrgpu_spinor_field_g5_mulc_add_assign(int par, int prec, void *s1, double c_re, double c_im, const void *s2);
+int hrgpu_spinor_field_mul(int par, int prec, void *s1, double r, const void *s2);
+int hrgpu_spinor_field_mulc(int par, int prec, void *s1, double c_re, double c_im, const void *s2);
+int hrgpu_spinor_field_add(int par, int prec, void *r, const void *s1, const void *s2);
+int hrgpu_spinor_field_sub(int par, int prec, void *r, const void *s1, const void *s2);
+int hrgpu_spinor_field_add_assign(int par, int prec, void *s1, const void *s2);
+int hrgpu_spinor_field_sub_assign(int par, int prec, void *s1, const void *s2);
+int hrgpu_spinor_field_copy(int par, int prec, void *s1, const void *s2);
+int hrgpu_spinor_field_zero(int par, int prec, void *s1);
+int hrgpu_spinor_field_minus(int par, int prec, void *s1, const void *s2);
+int hrgpu_spinor_field_lc(int par, int prec, void *s1, double r1, const void *s2, double r2, const void *s3);
+int hrgpu_spinor_field_lc_add_assign(int par, int prec, void *s1, double r1, const void *s2, double r2, const void *s3);
+int hrgpu_spinor_field_clc(int par, int prec, void *s1, double c1_re, double c1_im, const void *s2,
+                           double c2_re, double c2_im, const void *s3);
+int hrgpu_spinor_field_clc_add_assign(int par, int prec, void *s1, double c1_re, double c1_im, const void *s2,
+                                      double c2_re, double c2_im, const void *s3);
+int hrgpu_spinor_field_g5(int par, int prec, void *s1, const void *s2);
+int hrgpu_spinor_field_g5_assign(int par, int prec, void *s1);
+int hrgpu_spinor_field_g0(int par, int prec, void *s1, const void *s2);
+int hrgpu_spinor_field_g1(int par, int prec, void *s1, const void *s2);
+int hrgpu_spinor_field_g2(int par, int prec, void *s1, const void *s2);
+int hrgpu_spinor_field_g3(int par, int prec, void *s1, const void *s2);
+int hrgpu_spinor_field_lc1(int par, int prec, double c1, void *s1, const void *s2);
+int hrgpu_spinor_field_lc2(int par, int prec, double c1, double c2, void *s1, const void *s2);
+int hrgpu_spinor_field_lc3(int par, int prec, double c1, double c2, const void *s1, const void *s2, void *s3);
+
+/* ------------------------------------------------------------- inverters -- */
+/* cg_mshift (LibHR/Inverters/cg_mshift.c:147-195): out[i] = (M - shift[i])^-1 in,
+ * M selected by op at the given mass; err2 is HiRep's squared relative residual;
+ * with n == 1 out[0] is the initial guess.  *iters gets the MVM count as HiRep
+ * counts it (including the final true-residual checks). */
+int hrgpu_cg_mshift(int op, double mass, int n, const double *shift, double err2, int max_iter,
+                    const void *in, void *const *out, int *iters);
+/* cg_mshift_flt (LibHR/Inverters/cg_mshift_flt.c:144-276): FP64 defect correction
+ * around an FP32 multi-shift CG on the float twin of op (clover included). */
+int hrgpu_cg_mshift_flt(int op, double mass, int n, const double *shift, double err2, int max_iter,
+                        const void *in, void *const *out, int *iters);
+
+/* ----------------------------------------------------------------- force -- */
+int hrgpu_fermion_force_begin(void);                    /* force_fermion_core.c:935-962 */
+/* force_fermion_core (force_fermion_core.c:788-928, UPDATE_EO build): Xs, Ys are
+ * full-lattice device fields; with auto_fill_odd their odd halves are overwritten
+ * by D_oe (times D_oo^-1 with clover) of the even halves, as in the reference. */
+int hrgpu_force_fermion_core(void *Xs, void *Ys, int auto_fill_odd, double dt, double residue);
+int hrgpu_force_clover_logdet(double mass, double residue); /* force_fermion_core.c:777-781 */
+/* fermion_force_end (force_fermion_core.c:964-993): clover derivative, then adds the
+ * accumulated force to the host momentum field force[V][4][NG*NG-1] (HiRep layout) */
+int hrgpu_fermion_force_end(double dt, double *force_host);
+/* the accumulator itself, HiRep layout (for tests) */
+int hrgpu_force_sum_get(double *host);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
