@@ -1,0 +1,318 @@
+"""Benchmark of the even-odd clover Dirac operator and the FP64 / mixed-precision solves.
+
+Workload (the configuration the headline metric is quoted on): SU(3)
+fundamental, clover csw = 1.0, m0 = -0.2, lattice 16^3 x 32, smooth synthetic
+links U = exp(i 0.3 H) (seed 7, plaquette about 0.79), antiperiodic in time, a
+Gaussian FP64 source on the even sites.
+
+One step = one application of the even-odd preconditioned clover operator
+Cphi_eopre (= D_ee - D_eo D_oo^-1 D_oe), i.e. two launches of the fused hopping
+kernel.  value = GB/s under HiRep's own byte model
+(TestProgram/DiracOperator/speed_test_diracoperator.c:77-82: 36 vectors + 8
+links per site and hop) plus the clover blocks and the (4+m)^2 input read:
+    V * 2880 + V/2 * 192 + V/2 * (672 + 576) bytes per application.
+Inputs (126 MB working set) are below the L2 size, so a 512 MB buffer is
+written between timed steps to flush L2.  Times are CUDA events on the
+library's stream.
+
+Besides the step the run reports the time to |r|/|b| < 1e-12 (err2 = 1e-24) of
+the plain FP64 CG and of the FP32-inner defect-correction CG on g5Cphi_eopre^2,
+the end-to-end rate through the C ABI with host buffers, the roofline of the
+hopping kernel against the measured HBM copy bandwidth, and the CPU oracle on
+the host cores as a reported baseline.
+
+--impl reference times the CPU restatement of HiRep's operator (the reference
+itself needs generated headers and is not built here) on all host cores.
+With --gpus N (torchrun) every rank runs an independent replica on its own GPU
+(the single-GPU scope has no halo exchange); value is the sum over ranks and
+the time the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DIMS = (32, 16, 16, 16)  # T, X, Y, Z
+NG, MASS, CSW, EPS, SEED = 3, -0.2, 1.0, 0.3, 7
+SITE_BYTES = 2880  # 36 * sizeof(suNf_vector) + 8 * sizeof(suNf), SU(3) fundamental, double
+SPINOR_BYTES = 192
+CLOVER_BYTES = 672 + 576  # sizeof(ldl_t) + 4 * sizeof(suNfc), NF = 3
+ERR2 = 1e-24
+
+
+def eopre_bytes(V):
+    return V * SITE_BYTES + (V // 2) * SPINOR_BYTES + (V // 2) * CLOVER_BYTES
+
+
+def workload_config():
+    T, X, Y, Z = DIMS
+    return {"workload": "clover eopre Dslash + solve, SU(3) fund, 16^3x32, csw=1.0, m0=-0.2, U=exp(i0.3H) seed 7",
+            "lattice": f"{X}x{Y}x{Z}x{T}", "ng": NG, "repr": "fundamental", "nf": 3, "csw": CSW, "m0": MASS,
+            "l2": "512 MB buffer written between timed steps", "bytes_model": "HiRep speed_test byte model + clover blocks"}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the hopping kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "hop_clover_su3_16x16x16x32.txt")
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_eopre:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference_arm(args):
+    """The CPU restatement of HiRep's operator on all host cores (reference arm / cpu_baseline)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from hirep_b200 import fields as F
+
+    threads = os.cpu_count() or 1
+    o = O.Oracle(*DIMS, NG, O.FUND, threads=threads)
+    u = F.smooth_gauge(SEED, o.V, NG, EPS)
+    o.set_gauge(o.represent_gauge_field(u, True))
+    o.clover_init(CSW)
+    o.compute_clover_term()
+    src = F.gaussian_spinor(SEED, o.VH, o.nf)
+    o.Cphi_eopre(MASS, src)  # builds the LDL cache
+    times = []
+    t_end = time.perf_counter() + args.cpu_seconds
+    while len(times) < 3 or (time.perf_counter() < t_end and len(times) < 200):
+        t0 = time.perf_counter()
+        o.Cphi_eopre(MASS, src)
+        times.append(time.perf_counter() - t0)
+    t = float(np.median(times))
+    gbs = eopre_bytes(o.V) / t / 1e9
+    return {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
+            "sample": f"{len(times)} Cphi_eopre applications on 16^3x32 (median {t * 1e3:.1f} ms), OpenMP"}, t
+
+
+def reference_main(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    base, t = cpu_reference_arm(args)
+    line = {"impl": "reference", "metric": "eopre Dslash GB/s (HiRep byte model)", "value": base["value"],
+            "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": workload_config(), "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-solve", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return reference_main(args)
+
+    import torch
+
+    from hirep_b200 import fields as F
+    from hirep_b200 import hrgpu as G
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    lat = G.Lattice(*DIMS, NG, G.FUND, device=local)
+    u = F.smooth_gauge(SEED, lat.V, NG, EPS)
+    lat.set_gauge(u)
+    lat.represent_gauge_field(True)
+    lat.clover_init(CSW)
+    src = F.gaussian_spinor(SEED, lat.VH, lat.nf)
+    fin, fout = lat.field(G.EVEN, host=src), lat.field(G.EVEN)
+    nbytes = eopre_bytes(lat.V)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    for _ in range(args.warmup):
+        lat.Cphi_eopre(MASS, fout, fin)
+    torch.cuda.synchronize()
+    lat.getMVM()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        for a, b in evs:
+            flush.zero_()
+            a.record(stream)
+            lat.Cphi_eopre(MASS, fout, fin)
+            b.record(stream)
+        torch.cuda.synchronize()
+    launches = 2 * args.steps
+    step_ms = sum(a.elapsed_time(b) for a, b in evs) / args.steps
+    t_max = step_ms
+    if dist:
+        tt = torch.tensor([step_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    value = world * nbytes / (t_max * 1e-3) / 1e9
+
+    # end to end through the C ABI: host (pinned) -> device, operator, device -> host
+    h_in = torch.from_numpy(src.view(np.float64)).pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    h2d = d2h = lat.VH * SPINOR_BYTES
+    e2e = []
+    for k in range(args.warmup + args.steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        G._check(lat.L.hrgpu_spinor_upload(fin.ptr, G.ctypes.c_void_p(h_in.data_ptr()), G.EVEN, G.DOUBLE), "upload")
+        lat.Cphi_eopre(MASS, fout, fin)
+        G._check(lat.L.hrgpu_spinor_download(G.ctypes.c_void_p(h_out.data_ptr()), fout.ptr, G.EVEN, G.DOUBLE), "download")
+        b.record(stream)
+        torch.cuda.synchronize()
+        if k >= args.warmup:
+            e2e.append(a.elapsed_time(b))
+    e2e_ms = float(np.mean(e2e))
+    if dist:
+        tt = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+
+    solve = None
+    if not args.no_solve:
+        solve = run_solves(lat, fin, torch, stream, G, dist)
+
+    peak, peak_kind = measured_peak()
+    line = {
+        "metric": "eopre Dslash GB/s (%HBM peak); time to |r|/|b|<1e-12, mixed vs FP64 solve",
+        "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "config": workload_config(),
+        "roofline": {"bound": "hbm", "achieved": nbytes / (t_max * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": nbytes / (t_max * 1e-3) / 1e9 / peak, "peak_kind": peak_kind,
+                     "kernel": "k_hop (2 launches per Cphi_eopre)", "algorithmic_bytes_per_step": nbytes,
+                     "traffic": profile_traffic()},
+        "e2e": {"value": world * nbytes / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if solve:
+        line["solve"] = solve
+    if rank == 0 and world == 1 and not args.no_cpu:
+        base, _ = cpu_reference_arm(args)
+        line["cpu_baseline"] = base
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_solves(lat, fin, torch, stream, G, dist):
+    """Plain FP64 CG vs FP32-inner defect correction on g5Cphi_eopre^2, |r|/|b| < 1e-12."""
+    x64, x32 = lat.field(G.EVEN), lat.field(G.EVEN)
+    out = {}
+    for name, flt, x in (("fp64", False, x64), ("mixed", True, x32)):
+        times, iters = [], None
+        for rep in range(3):
+            lat.la("zero", x)
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            it, ok = lat.cg_mshift(G.OP_G5CPHI_EOPRE_SQ, MASS, [0.0], ERR2, fin, [x], flt=flt)
+            b.record(stream)
+            torch.cuda.synchronize()
+            if rep > 0:
+                times.append(a.elapsed_time(b))
+            iters = it
+        out[name + "_ms"] = float(np.median(times))
+        out[name + "_mvm"] = iters
+    r = lat.field(G.EVEN)
+    lat.g5Cphi_eopre_sq(MASS, r, x32)
+    lat.la("sub_assign", r, fin)
+    out["mixed_true_rel_residual"] = float(np.sqrt(lat.sqnorm(r) / lat.sqnorm(fin)))
+    lat.la("sub_assign", x32, x64)
+    out["mixed_vs_fp64_rel_error"] = float(np.sqrt(lat.sqnorm(x32) / lat.sqnorm(x64)))
+    out["speedup_mixed_vs_fp64"] = out["fp64_ms"] / out["mixed_ms"]
+    out["err2"] = ERR2
+    return out
+
+
+if __name__ == "__main__":
+    main()

@@ -280,7 +280,7 @@ int clover_prepare(double mass, int prec) {
     L.sigma_diag = sigma;
   }
   if (L.sigma != sigma) {
-    HR_NFC_DISPATCH(L.nf, (k_clover_pack_inv<N_><<<nb(n), 64, 0, L.stream>>>(L.cl_term, sigma, L.cl_idg, L.cl_iod, g)));
+    HR_NFC_DISPATCH(L.nf, (k_clover_pack_inv<N_><<<nb(n, 64), 64, 0, L.stream>>>(L.cl_term, sigma, L.cl_idg, L.cl_iod, g)));
     HR_LAUNCH_CHECK();
     L.sigma = sigma;
   }
