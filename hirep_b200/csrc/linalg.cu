@@ -179,7 +179,11 @@ int la_dot(int op, int par, int prec, const void *s1, const void *s2, double *re
   else
     k_dot<float2><<<grid, RED_THREADS, 0, L.stream>>>(op, (const float2 *)s1, (const float2 *)s2, n, L.ld, L.nf, L.partials);
   HR_LAUNCH_CHECK();
-  return finish_reduction(grid, 2, res);
+  double r[2];
+  if (int rc = finish_reduction(grid, 2, r)) return rc;
+  res[0] = r[0];
+  if (op != 2) res[1] = r[1];  // |s1|^2 callers pass room for one value
+  return 0;
 }
 
 }  // namespace hrgpu

@@ -13,7 +13,7 @@ int la_check(int par, int prec);
 // s1 <- op(s1, s2, s3; c1, c2)
 int la_op(int op, int par, int prec, void *s1, const void *s2, const void *s3, double c1r, double c1i, double c2r,
           double c2i);
-// op 0: <s1,s2> -> res[0..1] (re, im); 1: <g5 s1, s2>; 2: |s1|^2 -> res[0]
+// op 0: <s1,s2> -> res[0..1] (re, im); 1: <g5 s1, s2> -> res[0..1]; 2: |s1|^2 -> res[0] only
 int la_dot(int op, int par, int prec, const void *s1, const void *s2, double *res);
 
 }  // namespace hrgpu
