@@ -14,6 +14,7 @@ Lattice L;
 static std::string g_err;
 static int g_device = -1;
 static cudaStream_t g_own_stream = 0;
+static bool g_stream_chosen = false;
 
 void set_error(const char *fmt, ...) {
   char buf[512];
@@ -325,7 +326,7 @@ int hrgpu_init(int device) {
   HR_REQUIRE(device >= 0 && device < n, HRGPU_E_ARG, "hrgpu_init: device %d not present (%d devices)", device, n);
   HR_CUDA(cudaSetDevice(device));
   if (!g_own_stream) HR_CUDA(cudaStreamCreateWithFlags(&g_own_stream, cudaStreamNonBlocking));
-  if (!L.stream) L.stream = g_own_stream;
+  if (!L.stream && !g_stream_chosen) L.stream = g_own_stream;
   g_device = device;
   return 0;
 }
@@ -376,7 +377,11 @@ int hrgpu_geometry(int T, int X, int Y, int Z, int *ipt, int *iup, int *idn) {
 }
 
 int hrgpu_set_stream(void *s) {
-  L.stream = s ? (cudaStream_t)s : g_own_stream;
+  // NULL selects the legacy default stream (stream 0), which is what PyTorch's
+  // default stream reports; the library's own stream is used until this is called
+  if (L.stream) HR_CUDA(cudaStreamSynchronize(L.stream));
+  L.stream = (cudaStream_t)s;
+  g_stream_chosen = true;
   return 0;
 }
 

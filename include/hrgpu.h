@@ -69,7 +69,8 @@ const char *hrgpu_last_error(void);
 int hrgpu_nf(void);
 /* bytes of one device spinor field of the given parity and precision */
 size_t hrgpu_spinor_bytes(int par, int prec);
-/* all work is issued on this stream (default: the library's own stream) */
+/* all work is issued on this stream; NULL is the legacy default stream (stream 0).
+ * Until this is called the library uses a stream of its own. */
 int hrgpu_set_stream(void *cuda_stream);
 int hrgpu_synchronize(void);
 
