@@ -11,9 +11,10 @@ kernel.  value = GB/s under HiRep's own byte model
 (TestProgram/DiracOperator/speed_test_diracoperator.c:77-82: 36 vectors + 8
 links per site and hop) plus the clover blocks and the (4+m)^2 input read:
     V * 2880 + V/2 * 192 + V/2 * (672 + 576) bytes per application.
-Inputs (126 MB working set) are below the L2 size, so a 512 MB buffer is
-written between timed steps to flush L2.  Times are CUDA events on the
-library's stream.
+Each application touches about 190 MB, but one launch only about 130 MB,
+close to the 126 MB L2, so L2 is flushed between timed steps: a 512 MB buffer
+is written and then another 512 MB buffer is read, which leaves L2 holding
+clean lines of unrelated data.  Times are CUDA events on the library's stream.
 
 Besides the step the run reports the time to |r|/|b| < 1e-12 (err2 = 1e-24) of
 the plain FP64 CG and of the FP32-inner defect-correction CG on g5Cphi_eopre^2,
@@ -45,6 +46,7 @@ SITE_BYTES = 2880  # 36 * sizeof(suNf_vector) + 8 * sizeof(suNf), SU(3) fundamen
 SPINOR_BYTES = 192
 CLOVER_BYTES = 672 + 576  # sizeof(ldl_t) + 4 * sizeof(suNfc), NF = 3
 ERR2 = 1e-24
+METRIC = "eopre Dslash GB/s (%HBM peak); time to |r|/|b|<1e-12, mixed vs FP64 solve"
 
 
 def eopre_bytes(V):
@@ -55,7 +57,7 @@ def workload_config():
     T, X, Y, Z = DIMS
     return {"workload": "clover eopre Dslash + solve, SU(3) fund, 16^3x32, csw=1.0, m0=-0.2, U=exp(i0.3H) seed 7",
             "lattice": f"{X}x{Y}x{Z}x{T}", "ng": NG, "repr": "fundamental", "nf": 3, "csw": CSW, "m0": MASS,
-            "l2": "512 MB buffer written between timed steps", "bytes_model": "HiRep speed_test byte model + clover blocks"}
+            "l2": "flushed between timed steps (512 MB written, then 512 MB read)", "bytes_model": "HiRep speed_test byte model + clover blocks"}
 
 
 def measured_peak():
@@ -81,7 +83,7 @@ def profile_traffic():
 class Clocks:
     """nvidia-smi sampler running during the timed region."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
@@ -92,7 +94,7 @@ class Clocks:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -112,14 +114,19 @@ class Clocks:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        import datetime
+
         for ln in getattr(self, "lines", []):
             f = [x.strip() for x in ln.split(",")]
             try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
+                ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                if hasattr(self, "t0") and not (self.t0 - 0.05 <= ts <= self.t1 + 0.05):
+                    continue
+                sm.append(float(f[2]))
+                mx = float(f[3])
             except (ValueError, IndexError):
                 continue
-            for n, v in zip(names, f[5:9]):
+            for n, v in zip(names, f[6:10]):
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
@@ -157,7 +164,7 @@ def reference_main(args):
     if rank != 0:
         return
     base, t = cpu_reference_arm(args)
-    line = {"impl": "reference", "metric": "eopre Dslash GB/s (HiRep byte model)", "value": base["value"],
+    line = {"impl": "reference", "metric": METRIC, "value": base["value"],
             "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic", "config": workload_config(), "cpu_baseline": base,
@@ -168,7 +175,7 @@ def reference_main(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -205,6 +212,14 @@ def main():
     fin, fout = lat.field(G.EVEN, host=src), lat.field(G.EVEN)
     nbytes = eopre_bytes(lat.V)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    flush_rd = torch.ones(64 << 20, dtype=torch.float64, device="cuda")  # 512 MB, read after the write
+
+    def flush_l2():
+        # write 512 MB, then read 512 MB: L2 ends up holding clean lines of an
+        # unrelated buffer, so neither our data nor dirty flush data is left in it
+        flush.zero_()
+        flush_rd.sum()
+
     stream = torch.cuda.current_stream()
 
     for _ in range(args.warmup):
@@ -216,12 +231,15 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     with Clocks(local) as clk:
+        time.sleep(0.3)  # let the sampler start
+        clk.t0 = time.time()
         for a, b in evs:
-            flush.zero_()
+            flush_l2()
             a.record(stream)
             lat.Cphi_eopre(MASS, fout, fin)
             b.record(stream)
         torch.cuda.synchronize()
+        clk.t1 = time.time()
     launches = 2 * args.steps
     step_ms = sum(a.elapsed_time(b) for a, b in evs) / args.steps
     t_max = step_ms
@@ -236,8 +254,8 @@ def main():
     h_out = torch.empty_like(h_in).pin_memory()
     h2d = d2h = lat.VH * SPINOR_BYTES
     e2e = []
-    for k in range(args.warmup + args.steps):
-        flush.zero_()
+    for k in range(args.warmup + min(args.steps, 200)):
+        flush_l2()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         G._check(lat.L.hrgpu_spinor_upload(fin.ptr, G.ctypes.c_void_p(h_in.data_ptr()), G.EVEN, G.DOUBLE), "upload")
@@ -259,7 +277,7 @@ def main():
 
     peak, peak_kind = measured_peak()
     line = {
-        "metric": "eopre Dslash GB/s (%HBM peak); time to |r|/|b|<1e-12, mixed vs FP64 solve",
+        "metric": METRIC,
         "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic", "config": workload_config(),
@@ -270,6 +288,7 @@ def main():
         "e2e": {"value": world * nbytes / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
+        "hop_tuning": hop_tuning(lat, G),
         "clocks": clk.summary(),
     }
     if solve:
@@ -282,6 +301,21 @@ def main():
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def hop_tuning(lat, G):
+    """Variant the autotuner picked for each tuned (precision, epilogue), with its timings."""
+    out = {}
+    names = {0: "axpy", 1: "clover_inv", 2: "clover"}
+    for prec in (G.DOUBLE, G.FLOAT):
+        for ep in range(3):
+            chosen = G.ctypes.c_int(-1)
+            ms = (G.ctypes.c_float * 4)()
+            G._check(lat.L.hrgpu_hop_tuning(prec, ep, G.ctypes.byref(chosen), ms), "hop_tuning")
+            if chosen.value >= 0:
+                out[("f64" if prec == G.DOUBLE else "f32") + "_" + names[ep]] = {
+                    "variant": chosen.value, "us_per_launch": [round(1e3 * x, 2) for x in ms]}
+    return out
 
 
 def run_solves(lat, fin, torch, stream, G, dist):

@@ -4,6 +4,18 @@
 
 namespace hrgpu {
 
+template <typename R, int EP>
+int launch_ep(HopArgs<R> &a);  // hop_launch.cuh, instantiated in dirac_{d,f}_ep*.cu
+
+template <typename R>
+int launch_hop(int ep, HopArgs<R> &a) {
+  if (ep == EP_AXPY) return launch_ep<R, EP_AXPY>(a);
+  if (ep == EP_CLOV_INV) return launch_ep<R, EP_CLOV_INV>(a);
+  return launch_ep<R, EP_CLOV>(a);
+}
+template int launch_hop<double>(int, HopArgs<double> &);
+template int launch_hop<float>(int, HopArgs<float> &);
+
 static unsigned long g_mvm = 0;
 static double g_static_mass = 0.0;
 
@@ -206,6 +218,21 @@ int hrgpu_g5Dphi_sq_flt(double m0, void *out, const void *in) { return sq<float>
 int hrgpu_Dphi_eopre_flt(double m0, void *out, const void *in) { return Dphi_eo<float>(m0, out, in, HRGPU_EVEN, 0, nullptr); }
 int hrgpu_g5Dphi_eopre_flt(double m0, void *out, const void *in) { return Dphi_eo<float>(m0, out, in, HRGPU_EVEN, 1, nullptr); }
 int hrgpu_g5Dphi_eopre_sq_flt(double m0, void *out, const void *in) { return sq<float>(op_eo_f, m0, out, in, HRGPU_EVEN); }
+
+int hrgpu_set_hop_variant(int variant) {
+  HR_REQUIRE(variant >= -1 && variant < HOP_VARIANTS, HRGPU_E_ARG, "set_hop_variant: variant must be -1..%d",
+             HOP_VARIANTS - 1);
+  L.hop_force = variant;
+  return 0;
+}
+
+int hrgpu_hop_tuning(int prec, int epilogue, int *chosen, float *ms) {
+  HR_REQUIRE(prec >= 0 && prec <= 1 && epilogue >= 0 && epilogue <= 2 && chosen && ms, HRGPU_E_ARG,
+             "hop_tuning: bad arguments");
+  *chosen = L.hop_variant[prec][epilogue];
+  for (int v = 0; v < HOP_VARIANTS; v++) ms[v] = L.hop_tune_ms[prec][epilogue][v];
+  return 0;
+}
 
 unsigned long hrgpu_getMVM(void) {
   unsigned long r = g_mvm >> 1;

@@ -1,0 +1,6 @@
+// double-precision hopping kernels, epilogue 2 (split so the instantiations compile in parallel)
+#include "hop_launch.cuh"
+
+namespace hrgpu {
+template int launch_ep<double, 2>(HopArgs<double> &);
+}

@@ -165,8 +165,8 @@ __device__ __forceinline__ void clover_epilogue(V (&ra)[NA], V (&rb)[NA], const 
   }
 }
 
-template <int NFT, bool REAL, typename R, int EP>
-__global__ void __launch_bounds__(HOP_THREADS) k_hop(HopArgs<R> a) {
+template <int NFT, bool REAL, typename R, int EP, int MINB>
+__global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop(HopArgs<R> a) {
   typedef typename C2<R>::T V;
   typedef typename LinkE<REAL, R>::T E;
   constexpr int NA = NFT;
@@ -292,6 +292,170 @@ __global__ void __launch_bounds__(HOP_THREADS) k_hop(HopArgs<R> a) {
     }
   }
   if (a.red) block_partial<R>(nrm, a.red);
+}
+
+
+// ---------------------------------------------------------------------------
+// Spin-split variant: two threads per site.  Thread h (0 or 1) carries the
+// half-spinor projection that starts from spin component h: for direction mu
+// and sign s it forms hv = psi_h + f * psi_t (t the partner component of
+// (1 -/+ gamma_mu), f = +-1 or +-i), multiplies by U or U^+, adds the product
+// to output spin h, and adds conj(f) times it to a partial sum of output spin t.
+// The partial sums of spins 2 and 3 of the two threads are combined with one
+// lane shuffle at the end.  Each thread holds a third of the accumulators of
+// k_hop, so the register count (and with it the number of resident warps that
+// keep loads in flight) improves; links are loaded by both threads of a pair at
+// the same address (one transaction).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int partner_of(int mu, int h) { return (mu == 0 || mu == 3) ? 2 + h : 3 - h; }
+
+template <typename V>
+__device__ __forceinline__ V shfl_pair(V v) {
+  V r;
+  r.x = __shfl_xor_sync(0xffffffffu, v.x, 1);
+  r.y = __shfl_xor_sync(0xffffffffu, v.y, 1);
+  return r;
+}
+
+// z * v for z in {+1, -1, +i, -i}: (re, im) selector
+template <typename V>
+__device__ __forceinline__ V mul_unit(V v, int re, int im) {
+  V r;
+  if (im == 0) { r.x = re * v.x; r.y = re * v.y; }
+  else { r.x = -im * v.y; r.y = im * v.x; }
+  return r;
+}
+
+template <int NFT, bool REAL, typename R, int EP, int MINB>
+__global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop2(HopArgs<R> a) {
+  typedef typename C2<R>::T V;
+  typedef typename LinkE<REAL, R>::T E;
+  constexpr int NA = NFT;
+  const int nf = NFT;
+  const Geo g = a.g;
+  if (a.stop && *a.stop) return;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int h = tid & 1;
+  const bool active = (tid >> 1) < g.VH;
+  const int cb = active ? (tid >> 1) : g.VH - 1;
+  const int outp = a.outp, inp = outp ^ 1;
+  int t, x, y, z;
+  cb_to_coords(g, cb, outp, t, x, y, z);
+  const long ld = g.ld, lplane = 2L * g.ld;
+  const V *in = (const V *)a.in;
+  const E *U = (const E *)a.U;
+  const long nf2 = (long)nf * nf;
+  V rm[NA], p2[NA], p3[NA], hv[NA], ch[NA];
+#pragma unroll
+  for (int i = 0; i < NA; i++) rm[i] = p2[i] = p3[i] = cmk<V>(0.0, 0.0);
+  const long so = (long)outp * ld + cb;
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++) {
+    int tp = t, xp = x, yp = y, zp = z, tm = t, xm = x, ym = y, zm = z;
+    if (mu == 0) { tp = (t + 1 == g.T) ? 0 : t + 1; tm = (t == 0) ? g.T - 1 : t - 1; }
+    if (mu == 1) { xp = (x + 1 == g.X) ? 0 : x + 1; xm = (x == 0) ? g.X - 1 : x - 1; }
+    if (mu == 2) { yp = (y + 1 == g.Y) ? 0 : y + 1; ym = (y == 0) ? g.Y - 1 : y - 1; }
+    if (mu == 3) { zp = (z + 1 == g.Z) ? 0 : z + 1; zm = (z == 0) ? g.Z - 1 : z - 1; }
+    const E *Umu = U + (long)mu * nf2 * lplane;
+    const int pt = partner_of(mu, h);
+    // projection factor f for sign +: mu0: 1; mu1: i; mu2: (h ? -1 : 1); mu3: (h ? -i : i)
+    const int fre = (mu == 0) ? 1 : (mu == 2) ? (h ? -1 : 1) : 0;
+    const int fim = (mu == 1) ? 1 : (mu == 3) ? (h ? -1 : 1) : 0;
+#pragma unroll
+    for (int sgn = 0; sgn < 2; sgn++) {  // 0: forward, 1: backward
+      const int s = sgn ? -1 : 1;
+      const int cn = sgn ? coords_to_cb(g, tm, xm, ym, zm) : coords_to_cb(g, tp, xp, yp, zp);
+      const V *sp = in + cn;
+#pragma unroll
+      for (int i = 0; i < NA; i++) {
+        V a0 = ld_c(sp + (long)(h * nf + i) * ld);
+        V a1 = ld_c(sp + (long)(pt * nf + i) * ld);
+        hv[i] = cadd(a0, mul_unit(a1, s * fre, s * fim));
+      }
+      if (sgn == 0) link_mul<NA, false>(ch, hv, Umu, lplane, so, nf);
+      else link_mul<NA, true>(ch, hv, Umu, lplane, (long)inp * ld + cn, nf);
+      // reconstruction: output spin h += chi, output spin pt += conj(f) chi
+#pragma unroll
+      for (int i = 0; i < NA; i++) {
+        rm[i] = cadd(rm[i], ch[i]);
+        V c = mul_unit(ch[i], s * fre, -s * fim);
+        if (pt == 2) p2[i] = cadd(p2[i], c);
+        else p3[i] = cadd(p3[i], c);
+      }
+    }
+  }
+  // combine the partial sums of spins 2 and 3 over the thread pair
+#pragma unroll
+  for (int i = 0; i < NA; i++) {
+    p2[i] = cadd(p2[i], shfl_pair(p2[i]));
+    p3[i] = cadd(p3[i], shfl_pair(p3[i]));
+  }
+  const R ca = a.cacc;
+  double nrm = 0.0;
+  V *out = (V *)a.out + cb;
+  const R sg = a.g5 ? (R)-1 : (R)1;
+  if (EP == EP_AXPY) {
+    // thread h writes spins h and 2+h
+    const V *aux = (const V *)a.aux + cb;
+#pragma unroll
+    for (int i = 0; i < NA; i++) {
+      V o0 = cscale(ca, rm[i]), o1 = cscale(ca, h ? p3[i] : p2[i]);
+      if (aux != nullptr && a.caux != (R)0) {
+        rmac(o0, a.caux, ld_c(aux + (long)(h * nf + i) * ld));
+        rmac(o1, a.caux, ld_c(aux + (long)((2 + h) * nf + i) * ld));
+      }
+      o1 = cscale(sg, o1);
+      if (active) {
+        out[(long)(h * nf + i) * ld] = o0;
+        out[(long)((2 + h) * nf + i) * ld] = o1;
+      }
+      nrm += (double)o0.x * o0.x + (double)o0.y * o0.y + (double)o1.x * o1.x + (double)o1.y * o1.y;
+    }
+  } else {
+    // thread h applies clover block h: block 0 on spins (0,1), block 1 on spins (2,3)
+    V other[NA];
+#pragma unroll
+    for (int i = 0; i < NA; i++) other[i] = shfl_pair(rm[i]);
+    V xin[2 * NA], yout[2 * NA];
+    const long lp = 2L * g.ld, site = (long)outp * g.ld + cb;
+    const int n2 = 2 * nf, no = nf * (2 * nf - 1);
+#pragma unroll
+    for (int i = 0; i < NA; i++) {
+      V u0 = h ? p2[i] : rm[i];     // spin 2h
+      V u1 = h ? p3[i] : other[i];  // spin 2h+1
+      if (EP == EP_CLOV_INV) {
+        xin[i] = cscale(ca, u0);
+        xin[nf + i] = cscale(ca, u1);
+      } else {
+        const V *aux = (const V *)a.aux + cb;
+        xin[i] = ld_c(aux + (long)((2 * h) * nf + i) * ld);
+        xin[nf + i] = ld_c(aux + (long)((2 * h + 1) * nf + i) * ld);
+        hv[i] = u0;
+        ch[i] = u1;
+      }
+    }
+    herm_apply<NA>(yout, xin, a.cdg + (long)h * n2 * lp, a.cod + (long)h * no * lp, lp, site, nf);
+    const R sb = h ? sg : (R)1;
+#pragma unroll
+    for (int i = 0; i < NA; i++) {
+      V o0 = yout[i], o1 = yout[nf + i];
+      if (EP == EP_CLOV) {
+        o0 = cadd(cscale(ca, hv[i]), o0);
+        o1 = cadd(cscale(ca, ch[i]), o1);
+      }
+      o0 = cscale(sb, o0);
+      o1 = cscale(sb, o1);
+      if (active) {
+        out[(long)((2 * h) * nf + i) * ld] = o0;
+        out[(long)((2 * h + 1) * nf + i) * ld] = o1;
+      }
+      nrm += (double)o0.x * o0.x + (double)o0.y * o0.y + (double)o1.x * o1.x + (double)o1.y * o1.y;
+    }
+  }
+  if (a.red) {
+    if (!active) nrm = 0.0;
+    block_partial<R>(nrm, a.red);
+  }
 }
 
 }  // namespace hrgpu

@@ -285,3 +285,32 @@ def test_force_matches_oracle(ng, rep, clover):
     fo = o.fermion_force_end(0.7, mom)
     fg = lat.fermion_force_end(0.7, mom)
     assert rel(fg - mom, fo - mom) < 1e-12
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("ng,rep", [(3, O.FUND), (2, O.ADJ), (3, O.SYM)])
+def test_hop_variants(variant, ng, rep):
+    """Every variant of the hopping kernel the autotuner can pick gives the oracle's result."""
+    o, lat, _, _ = setup((4, 4, 6, 4), ng, rep, seed=21, smooth=0.3)
+    G._check(lat.L.hrgpu_set_hop_variant(variant), "set_hop_variant")
+    try:
+        m = -0.2
+        e = F.gaussian_spinor(5, o.VH, o.nf)
+        fe, out = lat.field(O.EVEN, host=e), lat.field(O.EVEN)
+        lat.g5Dphi_eopre(m, out, fe)
+        assert rel(out.download(), o.g5Dphi_eopre(m, e)) < TOL64
+        full = F.gaussian_spinor(6, o.V, o.nf)
+        ff, outf = lat.field(O.FULL, host=full), lat.field(O.FULL)
+        lat.g5Dphi(m, outf, ff)
+        assert rel(outf.download(), o.g5Dphi(m, full)) < TOL64
+        o.clover_init(1.0)
+        o.compute_clover_term()
+        lat.clover_init(1.0)
+        lat.g5Cphi_eopre(m, out, fe)
+        assert rel(out.download(), o.g5Cphi_eopre(m, e)) < TOL64
+        e32 = e.astype(np.complex64)
+        fe32, out32 = lat.field(O.EVEN, G.FLOAT, host=e32), lat.field(O.EVEN, G.FLOAT)
+        lat.g5Dphi_eopre_flt(m, out32, fe32)
+        assert rel(out32.download(), o.g5Dphi_eopre_flt(m, e32)) < 10 * TOL32
+    finally:
+        G._check(lat.L.hrgpu_set_hop_variant(-1), "set_hop_variant")
