@@ -3,15 +3,33 @@
 // compile in parallel.
 #pragma once
 #include "dirac.cuh"
+#include "hop_async.cuh"
 
 namespace hrgpu {
+
+template <int N, bool RL, typename R, int EP>
+int launch_async(HopArgs<R> &a, dim3 grid, dim3 block, cudaStream_t s) {
+  if constexpr (AsyncOK<N, RL>::v) {
+    constexpr int smem = AsyncLayout<N, RL, R>::SMEM;
+    static bool attr = false;
+    if (!attr) {
+      HR_CUDA(cudaFuncSetAttribute(k_hop_async<N, RL, R, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      attr = true;
+    }
+    k_hop_async<N, RL, R, EP><<<grid, block, smem, s>>>(a);
+    return 0;
+  } else {
+    return -1;  // not built for this NF
+  }
+}
 
 template <typename R, int EP>
 int launch_ep_variant(HopArgs<R> &a, int variant) {
   a.g = make_geo();
   a.nf = L.nf;
   // variants: 0 one thread per site, 1 two threads per site (spin split),
-  // 2 and 3 the same with the register budget capped for 4 resident blocks per SM
+  // 2 and 3 the same with the register budget capped for 4 resident blocks per SM,
+  // 4 one thread per site with the per-direction loads pipelined through shared memory
   const long threads = (variant & 1) ? 2L * L.VH : L.VH;
   dim3 grid((unsigned)((threads + HOP_THREADS - 1) / HOP_THREADS)), block(HOP_THREADS);
   cudaStream_t s = L.stream;
@@ -21,7 +39,10 @@ int launch_ep_variant(HopArgs<R> &a, int variant) {
       case 0: k_hop<N, RL, R, EP, 1><<<grid, block, 0, s>>>(a); break;                 \
       case 1: k_hop2<N, RL, R, EP, 1><<<grid, block, 0, s>>>(a); break;                \
       case 2: k_hop<N, RL, R, EP, 4><<<grid, block, 0, s>>>(a); break;                 \
-      default: k_hop2<N, RL, R, EP, 4><<<grid, block, 0, s>>>(a); break;               \
+      case 3: k_hop2<N, RL, R, EP, 4><<<grid, block, 0, s>>>(a); break;                \
+      default:                                                                         \
+        if (int rc_ = launch_async<N, RL, R, EP>(a, grid, block, s)) return rc_;       \
+        break;                                                                         \
     }                                                                                  \
     break;
 #define HOPC(N) HOPV(N, false)
@@ -45,7 +66,7 @@ int launch_ep_variant(HopArgs<R> &a, int variant) {
 }
 
 // Autotuner: the first launch of each (precision, epilogue) on a lattice times
-// both variants on the real arguments (3 launches each, CUDA events on the
+// every variant on the real arguments (3 launches each, CUDA events on the
 // library stream) and keeps the faster one.  The output is rewritten by the
 // final launch, so tuning does not change results.  hrgpu_set_hop_variant forces
 // a variant (tests use it to check both).
@@ -53,7 +74,14 @@ template <typename R, int EP>
 int launch_ep(HopArgs<R> &a) {
   const int pi = sizeof(R) == 8 ? 0 : 1;
   int &v = L.hop_variant[pi][EP];
-  if (L.hop_force >= 0) return launch_ep_variant<R, EP>(a, L.hop_force);
+  if (L.hop_force >= 0) {
+    int rc = launch_ep_variant<R, EP>(a, L.hop_force);
+    if (rc < 0) {
+      set_error("hopping-kernel variant %d is not built for NF=%d", L.hop_force, L.nf);
+      return HRGPU_E_NF;
+    }
+    return rc;
+  }
   if (v < 0) {
     float best = 1e30f;
     int bestv = 0;
@@ -61,7 +89,12 @@ int launch_ep(HopArgs<R> &a) {
     HR_CUDA(cudaEventCreate(&e0));
     HR_CUDA(cudaEventCreate(&e1));
     for (int cand = 0; cand < HOP_VARIANTS; cand++) {
-      if (int rc = launch_ep_variant<R, EP>(a, cand)) return rc;  // warm-up
+      int rc0 = launch_ep_variant<R, EP>(a, cand);  // warm-up
+      if (rc0 < 0) {  // variant not built for this NF
+        L.hop_tune_ms[pi][EP][cand] = -1.0f;
+        continue;
+      }
+      if (rc0) return rc0;
       HR_CUDA(cudaEventRecord(e0, L.stream));
       for (int r = 0; r < 3; r++)
         if (int rc = launch_ep_variant<R, EP>(a, cand)) return rc;
@@ -79,7 +112,12 @@ int launch_ep(HopArgs<R> &a) {
     cudaEventDestroy(e1);
     v = bestv;
   }
-  return launch_ep_variant<R, EP>(a, v);
+  int rc = launch_ep_variant<R, EP>(a, v);
+  if (rc < 0) {
+    set_error("hopping-kernel variant %d is not built for NF=%d", v, L.nf);
+    return HRGPU_E_NF;
+  }
+  return rc;
 }
 
 

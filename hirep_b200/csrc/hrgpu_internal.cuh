@@ -48,7 +48,7 @@ int fail_cuda(cudaError_t e, const char *what, const char *file, int line);
 constexpr int MAXNF = 64;
 constexpr int RED_THREADS = 256;
 constexpr int RED_MAX_BLOCKS = 1184;  // 8 x 148 SMs
-constexpr int HOP_VARIANTS = 4;
+constexpr int HOP_VARIANTS = 5;
 
 struct Lattice {
   bool ready = false;
@@ -95,7 +95,7 @@ struct Lattice {
   const int *cur_stop = nullptr;  // set by the inverters while they drive the operator
   int hop_variant[2][3] = {{-1, -1, -1}, {-1, -1, -1}};  // tuned hopping-kernel variant [prec][epilogue]
   int hop_force = -1;             // forced variant (-1: autotune)
-  float hop_tune_ms[2][3][4] = {};  // tuning times of the variants [prec][epilogue][variant]
+  float hop_tune_ms[2][3][HOP_VARIANTS] = {};  // tuning times of the variants [prec][epilogue][variant]
   cudaStream_t stream = 0;
   // temporaries (lazily allocated, sized for one parity unless noted)
   void *tmp_o = nullptr, *tmp_e = nullptr, *tmp_e2 = nullptr, *tmp_full = nullptr, *tmp_full2 = nullptr;

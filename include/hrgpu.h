@@ -118,8 +118,10 @@ int hrgpu_g5Dphi_eopre_flt(double m0, void *out, const void *in);
 int hrgpu_g5Dphi_eopre_sq_flt(double m0, void *out, const void *in);
 /* Hopping-kernel variant: 0 = one thread per site, 1 = two threads per site
  * (spin split), 2 and 3 = the same with registers capped for 4 blocks per SM,
- * -1 = autotune on first use (default).  hrgpu_hop_tuning reports the variant
- * chosen for (precision, epilogue 0..2) and the per-launch times it measured.
+ * 4 = one thread per site with cp.async-pipelined loads (NF <= 4 complex, NF = 3
+ * real), -1 = autotune on first use (default).  hrgpu_hop_tuning reports the
+ * variant chosen for (precision, epilogue 0..2) and the per-launch times it
+ * measured (ms has room for 5 values; -1 marks a variant not built for this NF).
  * Tuning controls of this library; they have no counterpart in the reference. */
 int hrgpu_set_hop_variant(int variant);
 int hrgpu_hop_tuning(int prec, int epilogue, int *chosen, float *ms);

@@ -287,7 +287,7 @@ def test_force_matches_oracle(ng, rep, clover):
     assert rel(fg - mom, fo - mom) < 1e-12
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("ng,rep", [(3, O.FUND), (2, O.ADJ), (3, O.SYM)])
 def test_hop_variants(variant, ng, rep):
     """Every variant of the hopping kernel the autotuner can pick gives the oracle's result."""
@@ -297,7 +297,12 @@ def test_hop_variants(variant, ng, rep):
         m = -0.2
         e = F.gaussian_spinor(5, o.VH, o.nf)
         fe, out = lat.field(O.EVEN, host=e), lat.field(O.EVEN)
-        lat.g5Dphi_eopre(m, out, fe)
+        try:
+            lat.g5Dphi_eopre(m, out, fe)
+        except G.HRGPUError as exc:
+            if "not built" in str(exc):
+                pytest.skip(f"variant {variant} is not built for NF={o.nf}")
+            raise
         assert rel(out.download(), o.g5Dphi_eopre(m, e)) < TOL64
         full = F.gaussian_spinor(6, o.V, o.nf)
         ff, outf = lat.field(O.FULL, host=full), lat.field(O.FULL)
