@@ -108,6 +108,15 @@ int hrgpu_Dphi_eopre(double m0, void *out, const void *in);       /* Dphi.c:874-
 int hrgpu_Dphi_oepre(double m0, void *out, const void *in);       /* Dphi.c:914-948   */
 int hrgpu_g5Dphi_eopre(double m0, void *out, const void *in);     /* Dphi.c:950-985   */
 int hrgpu_g5Dphi_eopre_sq(double m0, void *out, const void *in);  /* Dphi.c:988-998   */
+/* Dphi_eopre for callers that cannot let the library allocate device memory
+ * (a host framework that owns the GPU through its own memory pool).  Same
+ * result as hrgpu_Dphi_eopre, but the odd temporary lives in a 32 MiB static
+ * device array of the library instead of a cudaMalloc'd buffer; lattices whose
+ * odd FP64 field needs more are rejected with HRGPU_E_ARG.  The first call on a
+ * device looks up the array's address (make it before any stream capture); calls
+ * that overlap on the GPU share the array and race.  No counterpart in the
+ * reference. */
+int hrgpu_Dphi_eopre_noalloc(double m0, void *out, const void *in);
 /* single precision: LibHR/Update/Dphi_flt.c:162-593 */
 int hrgpu_Dphi_flt_(void *out, int out_par, const void *in);
 int hrgpu_Dphi_flt(double m0, void *out, const void *in);
