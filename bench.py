@@ -181,6 +181,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-solve", action="store_true")
+    ap.add_argument("--hop-variant", type=int, default=-1, help="hopping-kernel variant (-1: autotune)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -204,6 +205,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     lat = G.Lattice(*DIMS, NG, G.FUND, device=local)
+    G._check(lat.L.hrgpu_set_hop_variant(args.hop_variant), "set_hop_variant")
     u = F.smooth_gauge(SEED, lat.V, NG, EPS)
     lat.set_gauge(u)
     lat.represent_gauge_field(True)
