@@ -165,18 +165,16 @@ __device__ __forceinline__ void clover_epilogue(V (&ra)[NA], V (&rb)[NA], const 
   }
 }
 
-template <int NFT, bool REAL, typename R, int EP, int MINB>
-__global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop(HopArgs<R> a) {
+// one output site (checkerboard index cb < VH) of the hop; returns |out|^2 when a.red is set
+template <int NFT, bool REAL, typename R, int EP>
+__device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb) {
   typedef typename C2<R>::T V;
   typedef typename LinkE<REAL, R>::T E;
   constexpr int NA = NFT;
   const int nf = NFT;
   const Geo g = a.g;
-  if (a.stop && *a.stop) return;
-  const int cb = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool active = cb < g.VH;
   double nrm = 0.0;
-  if (active) {
+  {
     const int outp = a.outp, inp = outp ^ 1;
     int t, x, y, z;
     cb_to_coords(g, cb, outp, t, x, y, z);
@@ -291,7 +289,35 @@ __global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop(HopArgs<R> a) {
       }
     }
   }
+  return nrm;
+}
+
+template <int NFT, bool REAL, typename R, int EP, int MINB>
+__global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop(HopArgs<R> a) {
+  if (a.stop && *a.stop) return;
+  const int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  double nrm = 0.0;
+  if (cb < a.g.VH) nrm = hop_site<NFT, REAL, R, EP>(a, cb);
   if (a.red) block_partial<R>(nrm, a.red);
+}
+
+// Many right-hand sides at once: block = (32 sites) x (blockDim.y fields); the
+// fields of one batch are consecutive, fstride complex elements apart (in, out
+// and aux alike).  The warps of a block read the same links, so each link
+// crosses HBM once per block of sites instead of once per field.
+template <int NFT, bool REAL, typename R, int EP>
+__global__ void __launch_bounds__(HOP_THREADS) k_hop_batch(HopArgs<R> a, long fstride, int nrhs) {
+  typedef typename C2<R>::T V;
+  if (a.stop && *a.stop) return;
+  const int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  const int rhs = blockIdx.y * blockDim.y + threadIdx.y;
+  if (cb >= a.g.VH || rhs >= nrhs) return;
+  HopArgs<R> b = a;
+  b.in = (const V *)a.in + rhs * fstride;
+  b.out = (V *)a.out + rhs * fstride;
+  if (a.aux) b.aux = (const V *)a.aux + rhs * fstride;
+  b.red = nullptr;
+  hop_site<NFT, REAL, R, EP>(b, cb);
 }
 
 
