@@ -278,11 +278,13 @@ int clover_prepare(double mass, int prec) {
     HR_NFC_DISPATCH(L.nf, (k_clover_pack_diag<N_><<<nb(n), 128, 0, L.stream>>>(L.cl_term, sigma, L.cl_dg, L.cl_od, g)));
     HR_LAUNCH_CHECK();
     L.sigma_diag = sigma;
+    L.clover_gen[HRGPU_DOUBLE]++;
   }
   if (L.sigma != sigma) {
     HR_NFC_DISPATCH(L.nf, (k_clover_pack_inv<N_><<<nb(n, 64), 64, 0, L.stream>>>(L.cl_term, sigma, L.cl_idg, L.cl_iod, g)));
     HR_LAUNCH_CHECK();
     L.sigma = sigma;
+    L.clover_gen[HRGPU_DOUBLE]++;
   }
   if (prec == HRGPU_FLOAT && L.sigma_flt != sigma) {
     const long nd = 2L * 2 * L.nf * lp, no = 2L * L.nf * (2 * L.nf - 1) * lp * 2;
@@ -292,6 +294,7 @@ int clover_prepare(double mass, int prec) {
     k_cvt<float, double><<<nb(no, 256), 256, 0, L.stream>>>((float *)L.cl_iod_f, (const double *)L.cl_iod, no);
     HR_LAUNCH_CHECK();
     L.sigma_flt = sigma;
+    L.clover_gen[HRGPU_FLOAT]++;
   }
   return 0;
 }

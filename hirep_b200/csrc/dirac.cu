@@ -196,6 +196,8 @@ int op_parity(int op) { return (op == HRGPU_OP_G5DPHI_SQ || op == HRGPU_OP_G5CPH
 
 double static_mass() { return g_static_mass; }
 
+void add_mvm(unsigned long n) { g_mvm += n; }
+
 }  // namespace hrgpu
 
 using namespace hrgpu;

@@ -20,6 +20,8 @@ int Cphi_eo(double mass, void *out, const void *in, int g5, double *red);
 int apply_op(int op, int prec, double mass, void *out, const void *in);
 int op_parity(int op);
 double static_mass();
+void add_mvm(unsigned long n);  // hops done outside hop(), e.g. replayed CUDA graphs
+void batch_release();           // batch.cu: workspaces and captured graphs
 
 // clover: make sure the packed (4+m)+A blocks and their inverse exist for this
 // mass in this precision (the LDL cache of clover_tools.c:343-358)

@@ -131,11 +131,14 @@ __device__ __forceinline__ void block_partial(double v, double *red) {
 }
 
 // clover epilogue on one chiral block: (ra, rb) are the spin pair of block b
+// sofs / cs: offset of this site's first element and component stride in the
+// spinor fields (cb and ld for a single field)
 template <int NA, int EP, typename V, typename R>
-__device__ __forceinline__ void clover_epilogue(V (&ra)[NA], V (&rb)[NA], const HopArgs<R> &a, R ca, int cb, int b) {
+__device__ __forceinline__ void clover_epilogue(V (&ra)[NA], V (&rb)[NA], const HopArgs<R> &a, R ca, int cb, int b,
+                                                long sofs, long cs) {
   const Geo &g = a.g;
   const int nf = NA;
-  const long ld = g.ld, lp = 2L * g.ld, site = (long)a.outp * g.ld + cb;
+  const long lp = 2L * g.ld, site = (long)a.outp * g.ld + cb;
   const int n2 = 2 * nf, no = nf * (2 * nf - 1);
   V xin[2 * NA], yout[2 * NA];
   if (EP == EP_CLOV_INV) {
@@ -145,11 +148,11 @@ __device__ __forceinline__ void clover_epilogue(V (&ra)[NA], V (&rb)[NA], const 
       xin[nf + i] = cscale(ca, rb[i]);
     }
   } else {
-    const V *aux = (const V *)a.aux + cb;
+    const V *aux = (const V *)a.aux + sofs;
 #pragma unroll
     for (int i = 0; i < NA; i++) {
-      xin[i] = ld_c(aux + (long)((2 * b) * nf + i) * ld);
-      xin[nf + i] = ld_c(aux + (long)((2 * b + 1) * nf + i) * ld);
+      xin[i] = ld_c(aux + (long)((2 * b) * nf + i) * cs);
+      xin[nf + i] = ld_c(aux + (long)((2 * b + 1) * nf + i) * cs);
     }
   }
   herm_apply<NA>(yout, xin, a.cdg + (long)b * n2 * lp, a.cod + (long)b * no * lp, lp, site, nf);
@@ -185,7 +188,7 @@ __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb) {
     V r0[NA], r1[NA], r2[NA], r3[NA], h0[NA], h1[NA], c0[NA], c1[NA];
 #pragma unroll
     for (int i = 0; i < NA; i++) r0[i] = r1[i] = r2[i] = r3[i] = cmk<V>(0.0, 0.0);
-    const long so = (long)outp * ld + cb;  // this site in the link planes
+    const long so = (long)outp * g.ld + cb;  // this site in the link planes
 #pragma unroll
     for (int mu = 0; mu < 4; mu++) {
       int tp = t, xp = x, yp = y, zp = z, tm = t, xm = x, ym = y, zm = z;
@@ -235,7 +238,7 @@ __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb) {
           if (mu == 2) { h0[i] = csub(s0, s3); h1[i] = cadd(s1, s2); }
           if (mu == 3) { h0[i] = csubi(s0, s2); h1[i] = caddi(s1, s3); }
         }
-        const long sn = (long)inp * ld + cdn;
+        const long sn = (long)inp * g.ld + cdn;
         link_mul<NA, true>(c0, h0, Umu, lplane, sn, nf);
         link_mul<NA, true>(c1, h1, Umu, lplane, sn, nf);
 #pragma unroll
@@ -270,8 +273,8 @@ __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb) {
       }
     } else {
       // clover blocks: block 0 acts on spin (0,1), block 1 on spin (2,3)
-      clover_epilogue<NA, EP>(r0, r1, a, ca, cb, 0);
-      clover_epilogue<NA, EP>(r2, r3, a, ca, cb, 1);
+      clover_epilogue<NA, EP>(r0, r1, a, ca, cb, 0, cb, ld);
+      clover_epilogue<NA, EP>(r2, r3, a, ca, cb, 1, cb, ld);
     }
     const R sg = a.g5 ? (R)-1 : (R)1;
 #pragma unroll
@@ -300,26 +303,6 @@ __global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop(HopArgs<R> a) {
   if (cb < a.g.VH) nrm = hop_site<NFT, REAL, R, EP>(a, cb);
   if (a.red) block_partial<R>(nrm, a.red);
 }
-
-// Many right-hand sides at once: block = (32 sites) x (blockDim.y fields); the
-// fields of one batch are consecutive, fstride complex elements apart (in, out
-// and aux alike).  The warps of a block read the same links, so each link
-// crosses HBM once per block of sites instead of once per field.
-template <int NFT, bool REAL, typename R, int EP>
-__global__ void __launch_bounds__(HOP_THREADS) k_hop_batch(HopArgs<R> a, long fstride, int nrhs) {
-  typedef typename C2<R>::T V;
-  if (a.stop && *a.stop) return;
-  const int cb = blockIdx.x * blockDim.x + threadIdx.x;
-  const int rhs = blockIdx.y * blockDim.y + threadIdx.y;
-  if (cb >= a.g.VH || rhs >= nrhs) return;
-  HopArgs<R> b = a;
-  b.in = (const V *)a.in + rhs * fstride;
-  b.out = (V *)a.out + rhs * fstride;
-  if (a.aux) b.aux = (const V *)a.aux + rhs * fstride;
-  b.red = nullptr;
-  hop_site<NFT, REAL, R, EP>(b, cb);
-}
-
 
 // ---------------------------------------------------------------------------
 // Spin-split variant: two threads per site.  Thread h (0 or 1) carries the
@@ -352,18 +335,15 @@ __device__ __forceinline__ V mul_unit(V v, int re, int im) {
   return r;
 }
 
-template <int NFT, bool REAL, typename R, int EP, int MINB>
-__global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop2(HopArgs<R> a) {
+// one thread (half h of the pair) of site cb; inactive threads compute but do
+// not write (their partner needs the shuffles)
+template <int NFT, bool REAL, typename R, int EP>
+__device__ __forceinline__ double hop2_site(const HopArgs<R> &a, const int cb, const int h, const bool active) {
   typedef typename C2<R>::T V;
   typedef typename LinkE<REAL, R>::T E;
   constexpr int NA = NFT;
   const int nf = NFT;
   const Geo g = a.g;
-  if (a.stop && *a.stop) return;
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int h = tid & 1;
-  const bool active = (tid >> 1) < g.VH;
-  const int cb = active ? (tid >> 1) : g.VH - 1;
   const int outp = a.outp, inp = outp ^ 1;
   int t, x, y, z;
   cb_to_coords(g, cb, outp, t, x, y, z);
@@ -374,7 +354,7 @@ __global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop2(HopArgs<R> a) {
   V rm[NA], p2[NA], p3[NA], hv[NA], ch[NA];
 #pragma unroll
   for (int i = 0; i < NA; i++) rm[i] = p2[i] = p3[i] = cmk<V>(0.0, 0.0);
-  const long so = (long)outp * ld + cb;
+  const long so = (long)outp * g.ld + cb;
 #pragma unroll
   for (int mu = 0; mu < 4; mu++) {
     int tp = t, xp = x, yp = y, zp = z, tm = t, xm = x, ym = y, zm = z;
@@ -399,7 +379,7 @@ __global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop2(HopArgs<R> a) {
         hv[i] = cadd(a0, mul_unit(a1, s * fre, s * fim));
       }
       if (sgn == 0) link_mul<NA, false>(ch, hv, Umu, lplane, so, nf);
-      else link_mul<NA, true>(ch, hv, Umu, lplane, (long)inp * ld + cn, nf);
+      else link_mul<NA, true>(ch, hv, Umu, lplane, (long)inp * g.ld + cn, nf);
       // reconstruction: output spin h += chi, output spin pt += conj(f) chi
 #pragma unroll
       for (int i = 0; i < NA; i++) {
@@ -478,10 +458,17 @@ __global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop2(HopArgs<R> a) {
       nrm += (double)o0.x * o0.x + (double)o0.y * o0.y + (double)o1.x * o1.x + (double)o1.y * o1.y;
     }
   }
-  if (a.red) {
-    if (!active) nrm = 0.0;
-    block_partial<R>(nrm, a.red);
-  }
+  return active ? nrm : 0.0;
+}
+
+template <int NFT, bool REAL, typename R, int EP, int MINB>
+__global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop2(HopArgs<R> a) {
+  if (a.stop && *a.stop) return;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = (tid >> 1) < a.g.VH;
+  const int cb = active ? (tid >> 1) : a.g.VH - 1;
+  double nrm = hop2_site<NFT, REAL, R, EP>(a, cb, tid & 1, active);
+  if (a.red) block_partial<R>(nrm, a.red);
 }
 
 }  // namespace hrgpu

@@ -181,8 +181,8 @@ __global__ void __launch_bounds__(HOP_THREADS) k_hop_async(HopArgs<R> a) {
       r0[i] = q0; r1[i] = q1; r2[i] = q2; r3[i] = q3;
     }
   } else {
-    clover_epilogue<NA, EP>(r0, r1, a, ca, cb, 0);
-    clover_epilogue<NA, EP>(r2, r3, a, ca, cb, 1);
+    clover_epilogue<NA, EP>(r0, r1, a, ca, cb, 0, cb, ld);
+    clover_epilogue<NA, EP>(r2, r3, a, ca, cb, 1, cb, ld);
   }
   const R sg = a.g5 ? (R)-1 : (R)1;
   double nrm = 0.0;

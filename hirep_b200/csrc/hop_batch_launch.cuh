@@ -1,0 +1,83 @@
+// hop_batch_launch.cuh -- host-side dispatch of the batch hopping kernel
+// (k_hopt) over NF and variant, with its autotuner; instantiated per precision
+// and epilogue in dirac_b_*.cu.
+#pragma once
+#include "dirac.cuh"
+#include "hop_tile.cuh"
+
+namespace hrgpu {
+
+// variants: the register budget for 1, 3 or 4 resident blocks of 128 threads per SM
+template <typename R, int EP>
+int launch_batch_variant(TileArgs<R> &a, int variant) {
+  a.g = make_geo();
+  // 32 threads per (group of 8 sites, tile)
+  const long threads = ((L.VH + TILE_S - 1) / TILE_S) * 32L * ((a.nb + TILE_F - 1) / TILE_F);
+  dim3 grid((unsigned)((threads + HOPT_THREADS - 1) / HOPT_THREADS)), block(HOPT_THREADS);
+  cudaStream_t s = L.stream;
+#define HOPTV(N, RL)                                                       \
+  case N:                                                                  \
+    switch (variant) {                                                     \
+      case 0: k_hopt<N, RL, R, EP, 1><<<grid, block, 0, s>>>(a); break;     \
+      case 1: k_hopt<N, RL, R, EP, 3><<<grid, block, 0, s>>>(a); break;     \
+      default: k_hopt<N, RL, R, EP, 4><<<grid, block, 0, s>>>(a); break;    \
+    }                                                                      \
+    break;
+  if (!L.real) {
+    switch (L.nf) {
+      HOPTV(2, false) HOPTV(3, false) HOPTV(4, false) HOPTV(5, false) HOPTV(6, false) HOPTV(10, false)
+      default: set_error("no batch hopping kernel for complex NF=%d", L.nf); return HRGPU_E_NF;
+    }
+  } else {
+    switch (L.nf) {
+      HOPTV(3, true) HOPTV(8, true) HOPTV(15, true)
+      default: set_error("no batch hopping kernel for real NF=%d", L.nf); return HRGPU_E_NF;
+    }
+  }
+#undef HOPTV
+  HR_LAUNCH_CHECK();
+  return 0;
+}
+
+// Autotuner: the first launch for a (precision, epilogue, nb) times every
+// variant (3 launches each after a warm-up, CUDA events on the library stream)
+// and keeps the fastest; the final launch rewrites the output, so tuning does
+// not change results.  While the stream is being captured into a CUDA graph
+// nothing can be timed: an untuned case then runs variant 0 untuned.
+template <typename R, int EP>
+int launch_batch(TileArgs<R> &a) {
+  const int pi = sizeof(R) == 8 ? 0 : 1;
+  if (L.hopb_force >= 0) return launch_batch_variant<R, EP>(a, L.hopb_force);
+  signed char &v = L.hopb_variant[pi][EP][a.nb];
+  if (v == 0) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    HR_CUDA(cudaStreamIsCapturing(L.stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return launch_batch_variant<R, EP>(a, 0);
+    float best = 1e30f;
+    int bestv = 0;
+    cudaEvent_t e0, e1;
+    HR_CUDA(cudaEventCreate(&e0));
+    HR_CUDA(cudaEventCreate(&e1));
+    for (int cand = 0; cand < HOPB_VARIANTS; cand++) {
+      if (int rc = launch_batch_variant<R, EP>(a, cand)) return rc;
+      HR_CUDA(cudaEventRecord(e0, L.stream));
+      for (int r = 0; r < 3; r++)
+        if (int rc = launch_batch_variant<R, EP>(a, cand)) return rc;
+      HR_CUDA(cudaEventRecord(e1, L.stream));
+      HR_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      HR_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      L.hopb_tune_ms[pi][EP][a.nb][cand] = ms / 3.0f;
+      if (ms < best) {
+        best = ms;
+        bestv = cand;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    v = (signed char)(bestv + 1);
+  }
+  return launch_batch_variant<R, EP>(a, v - 1);
+}
+
+}  // namespace hrgpu

@@ -49,6 +49,8 @@ constexpr int MAXNF = 64;
 constexpr int RED_THREADS = 256;
 constexpr int RED_MAX_BLOCKS = 1184;  // 8 x 148 SMs
 constexpr int HOP_VARIANTS = 5;
+constexpr int HOPB_VARIANTS = 3;   // batch hopping kernel variants
+constexpr int HOPB_MAXNB = 64;     // fields per batch
 
 struct Lattice {
   bool ready = false;
@@ -96,6 +98,13 @@ struct Lattice {
   int hop_variant[2][3] = {{-1, -1, -1}, {-1, -1, -1}};  // tuned hopping-kernel variant [prec][epilogue]
   int hop_force = -1;             // forced variant (-1: autotune)
   float hop_tune_ms[2][3][HOP_VARIANTS] = {};  // tuning times of the variants [prec][epilogue][variant]
+  // multi-field kernel: tuned variant + 1 (0 = not tuned yet) [prec][epilogue][nb], its timings, forced variant
+  signed char hopb_variant[2][3][HOPB_MAXNB + 1] = {};
+  float hopb_tune_ms[2][3][HOPB_MAXNB + 1][HOPB_VARIANTS] = {};
+  int hopb_force = -1;
+  // change counters: links (double and float are rewritten together) and the
+  // packed clover blocks of each precision; copies made from them record these
+  unsigned long gauge_gen = 0, clover_gen[2] = {0, 0};
   cudaStream_t stream = 0;
   // temporaries (lazily allocated, sized for one parity unless noted)
   void *tmp_o = nullptr, *tmp_e = nullptr, *tmp_e2 = nullptr, *tmp_full = nullptr, *tmp_full2 = nullptr;

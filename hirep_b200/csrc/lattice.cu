@@ -551,6 +551,7 @@ int hrgpu_assign_ud2u_f(void) {
   k_convert<float, double><<<nblk(n), 256, 0, L.stream>>>((float *)L.Uf, (const double *)L.U, n);
   HR_LAUNCH_CHECK();
   L.have_gauge_flt = true;
+  L.gauge_gen++;  // every write of the double links is followed by this call
   return 0;
 }
 

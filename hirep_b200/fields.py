@@ -64,3 +64,13 @@ def gaussian_spinor(seed, nsites, nf, dtype=np.complex128):
 
 def nf_of(ng, repr_name):
     return {"FUND": ng, "ADJ": ng * ng - 1, "SYM": ng * (ng + 1) // 2, "ASYM": ng * (ng - 1) // 2}[repr_name]
+
+
+def point_source(nsites, nf, spin, col, site=0, dtype=np.complex128):
+    """One spin-colour point source: 1 at component (spin, col) of one site, in
+    HiRep's site order (site 0 = the origin, an even site).  HiRep's
+    create_full_point_source (LibHR/Observables/sources.c:114-140) fills source
+    index spin + 4*col this way at timeslice tau."""
+    a = np.zeros((nsites, 4, nf), dtype)
+    a[site, spin, col] = 1.0
+    return a

@@ -18,6 +18,7 @@ EVEN, ODD, FULL = 0, 1, 2
 DOUBLE, FLOAT = 0, 1
 FUND, ADJ, SYM, ASYM = 0, 1, 2, 3
 OP_G5DPHI_SQ, OP_G5DPHI_EOPRE_SQ, OP_G5CPHI_EOPRE_SQ, OP_G5CPHI_SQ = 0, 1, 2, 3
+OP_DPHI_EOPRE, OP_G5DPHI_EOPRE, OP_CPHI_EOPRE, OP_G5CPHI_EOPRE = 4, 5, 6, 7
 E_NOCONV = 5
 
 _lib = None
@@ -37,6 +38,7 @@ def lib():
         L.hrgpu_spinor_bytes.restype = ctypes.c_size_t
         L.hrgpu_getMVM.restype = ctypes.c_ulong
         L.hrgpu_get_dirac_mass.restype = ctypes.c_double
+        L.hrgpu_batch_bytes.restype = ctypes.c_size_t
         _lib = L
     return _lib
 
@@ -87,6 +89,31 @@ class Field:
         out = np.empty((self.lat.nsites(self.par), 4, self.lat.nf), dt)
         _check(lib().hrgpu_spinor_download(_ptr(out), self.ptr, self.par, self.prec), "spinor_download")
         return out
+
+
+class Batch:
+    """nb even-parity fields interleaved in one device buffer (field index fastest)."""
+
+    def __init__(self, lat, nb, prec=DOUBLE):
+        import torch
+
+        self.lat, self.nb, self.prec = lat, nb, prec
+        self.nbytes = lib().hrgpu_batch_bytes(prec, nb)
+        if self.nbytes == 0:
+            raise HRGPUError("batch_bytes: lattice not initialised or nb <= 0")
+        self.buf = torch.zeros(self.nbytes, dtype=torch.uint8, device="cuda")
+        self.ptr = ctypes.c_void_p(self.buf.data_ptr())
+
+    def pack(self, fields):
+        assert len(fields) == self.nb
+        arr = (ctypes.c_void_p * self.nb)(*[f.ptr.value for f in fields])
+        _check(lib().hrgpu_batch_pack(self.ptr, arr, self.nb, self.prec), "batch_pack")
+        return self
+
+    def unpack(self, fields):
+        assert len(fields) == self.nb
+        arr = (ctypes.c_void_p * self.nb)(*[f.ptr.value for f in fields])
+        _check(lib().hrgpu_batch_unpack(arr, self.ptr, self.nb, self.prec), "batch_unpack")
 
 
 class Lattice:
@@ -249,6 +276,33 @@ class Lattice:
             return it.value, False
         _check(rc, "cg_mshift_flt" if flt else "cg_mshift")
         return it.value, True
+
+    # many right-hand sides -------------------------------------------------------
+    def batch(self, nb, prec=DOUBLE, fields=None):
+        b = Batch(self, nb, prec)
+        if fields is not None:
+            b.pack(fields)
+        return b
+
+    def apply_op_batch(self, op, mass, out, inp):
+        _check(self.L.hrgpu_apply_op_batch(op, out.prec, D(mass), out.ptr, inp.ptr, out.nb), "apply_op_batch")
+
+    def cg_mshift_batch(self, op, mass, sources, shifts, err2, outs, max_iter=0, flt=False):
+        """sources: list of even Fields; shifts: list (per source) of shift lists;
+        outs: flat list of Fields, source by source.  Returns (iters per source, ok)."""
+        nsrc = len(sources)
+        nsh = np.ascontiguousarray([len(s) for s in shifts], np.int32)
+        sh = np.ascontiguousarray([x for s in shifts for x in s], np.float64)
+        assert len(outs) == len(sh)
+        ins = (ctypes.c_void_p * nsrc)(*[f.ptr.value for f in sources])
+        arr = (ctypes.c_void_p * len(outs))(*[o.ptr.value for o in outs])
+        it = np.zeros(nsrc, np.int32)
+        rc = self.L.hrgpu_cg_mshift_batch(op, D(mass), nsrc, _ptr(nsh), _ptr(sh), D(err2), max_iter, ins, arr,
+                                          int(bool(flt)), _ptr(it))
+        if rc == E_NOCONV:
+            return it, False
+        _check(rc, "cg_mshift_batch")
+        return it, True
 
     # force -------------------------------------------------------------------
     def fermion_force_begin(self):

@@ -40,7 +40,12 @@ enum {
   HRGPU_OP_G5DPHI_SQ = 0,       /* g5Dphi_sq(mass)        Dphi.c:1001-1019, full lattice   */
   HRGPU_OP_G5DPHI_EOPRE_SQ = 1, /* g5Dphi_eopre_sq(mass)  Dphi.c:988-998, even sites       */
   HRGPU_OP_G5CPHI_EOPRE_SQ = 2, /* g5Cphi_eopre_sq(mass)  Dphi.c:1263-1272, even sites     */
-  HRGPU_OP_G5CPHI_SQ = 3        /* g5Cphi_sq(mass)        Dphi.c:1226-1235, full lattice   */
+  HRGPU_OP_G5CPHI_SQ = 3,       /* g5Cphi_sq(mass)        Dphi.c:1226-1235, full lattice   */
+  /* not positive: hrgpu_apply_op_batch only */
+  HRGPU_OP_DPHI_EOPRE = 4,      /* Dphi_eopre(mass)       Dphi.c:874-907                   */
+  HRGPU_OP_G5DPHI_EOPRE = 5,    /* g5Dphi_eopre(mass)     Dphi.c:950-985                   */
+  HRGPU_OP_CPHI_EOPRE = 6,      /* Cphi_eopre(mass)       Dphi.c:1240-1255                 */
+  HRGPU_OP_G5CPHI_EOPRE = 7     /* g5Cphi_eopre(mass)     Dphi.c:1257-1261                 */
 };
 /* status codes */
 enum {
@@ -214,6 +219,50 @@ int hrgpu_cg_mshift(int op, double mass, int n, const double *shift, double err2
  * around an FP32 multi-shift CG on the float twin of op (clover included). */
 int hrgpu_cg_mshift_flt(int op, double mass, int n, const double *shift, double err2, int max_iter,
                         const void *in, void *const *out, int *iters);
+
+/* ------------------------------------------------------ batched (multi-RHS) -- */
+/* HiRep has no batched interface; these entry points serve its callers that
+ * hold many sources at once (calc_prop.c:210-289 loops cg_mshift over the 4*NF
+ * spin-colour point sources; force_rhmc.c:24-112 solves one source for many
+ * shifts).  A batch of nb even-parity fields is one device buffer in tiles of 4
+ * fields (the last tile padded) and blocks of 8 sites: element (component c,
+ * site n, field f) at
+ *   (((f/4) * ld/8 + n/8) * 4NF + c) * 32 + (n%8) * 4 + f%4,
+ * where a single field has its element (c, n) at c*ld + n (ld: a multiple of 32).  hrgpu_batch_bytes
+ * gives its size (0 if not initialised or nb <= 0).  pack/unpack move nb
+ * separate device fields (the layout of hrgpu_spinor_upload) into a batch and
+ * back; nb <= 64. */
+size_t hrgpu_batch_bytes(int prec, int nb);
+int hrgpu_batch_pack(void *batch, const void *const *fields, int nb, int prec);
+int hrgpu_batch_unpack(void *const *fields, const void *batch, int nb, int prec);
+/* one even-odd operator (HRGPU_OP_G5DPHI_EOPRE_SQ, _G5CPHI_EOPRE_SQ, _DPHI_EOPRE,
+ * _G5DPHI_EOPRE, _CPHI_EOPRE, _G5CPHI_EOPRE) on every field of a batch; the
+ * result of each field is that of the single-field operator, to rounding. */
+int hrgpu_apply_op_batch(int op, int prec, double mass, void *out, const void *in, int nb);
+/* batch hopping kernel variants (one thread per site and field; 0, 1, 2: the
+ * register budget of 1, 3, 4 resident blocks per SM): -1 (default) autotunes
+ * per precision, epilogue and nb at first use; hrgpu_batch_tuning reports the
+ * choice (-1: not tuned yet) and the tuning times in ms (3 entries). */
+int hrgpu_set_batch_variant(int variant);
+int hrgpu_batch_tuning(int prec, int epilogue, int nb, int *chosen, float *ms);
+/* cg_mshift for many sources at once (op: g5Dphi_eopre_sq or g5Cphi_eopre_sq).
+ * Source s (in[s], a separate FP64 even field) is solved for its nshift[s]
+ * shifts: with o_s = nshift[0] + ... + nshift[s-1], out[o_s + i] =
+ * (M - shift[o_s + i])^-1 in[s], every system from a zero start (unlike
+ * hrgpu_cg_mshift with n == 1).  nsrc <= 32, total systems <= 64.  One Krylov
+ * space per source (the multi-shift recursion of cg_mshift.c:24-145), all
+ * sources advanced by one batched operator per iteration, the iteration replayed
+ * from a captured CUDA graph.  flt = 0: FP64 throughout, then HiRep's true
+ * residual check and single-shift restarts (cg_mshift.c:122-179); flt = 1:
+ * FP64 defect correction around batched FP32 solves.  Its first round is
+ * cg_mshift_flt's (cg_mshift_flt.c:144-276): one multi-shift solve per source;
+ * later rounds correct every unconverged system from its own residual (one
+ * single-shift Krylov space each), because after an FP32 solve the residuals of
+ * different shifts are collinear only up to FP32 noise.  iters[s] (nsrc
+ * entries) gets the batched iterations in which source s had a system running,
+ * plus its residual evaluations. */
+int hrgpu_cg_mshift_batch(int op, double mass, int nsrc, const int *nshift, const double *shift, double err2,
+                          int max_iter, const void *const *in, void *const *out, int flt, int *iters);
 
 /* ----------------------------------------------------------------- force -- */
 int hrgpu_fermion_force_begin(void);                    /* force_fermion_core.c:935-962 */
