@@ -181,6 +181,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-solve", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched 22-system solve (24^3x48 sextet)")
     ap.add_argument("--hop-variant", type=int, default=-1, help="hopping-kernel variant (-1: autotune)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -295,6 +296,8 @@ def main():
     }
     if solve:
         line["solve"] = solve
+    if world == 1 and not args.no_batch:
+        line["solve_batch"] = run_batch_solves(torch, stream, G, F)
     if rank == 0 and world == 1 and not args.no_cpu:
         base, _ = cpu_reference_arm(args)
         line["cpu_baseline"] = base
@@ -347,6 +350,89 @@ def run_solves(lat, fin, torch, stream, G, dist):
     out["mixed_vs_fp64_rel_error"] = float(np.sqrt(lat.sqnorm(x32) / lat.sqnorm(x64)))
     out["speedup_mixed_vs_fp64"] = out["fp64_ms"] / out["mixed_ms"]
     out["err2"] = ERR2
+    return out
+
+
+# batched workload: SU(3) two-index symmetric (NF = 6), clover csw = 1.0, m0 = -0.3,
+# 24^3 x 48, U = exp(i 0.3 H) seed 21; the 12 spin-colour point sources at the
+# origin (colours 0-2 x 4 spins), source 0 also for 10 shifts sigma log-spaced
+# 1e-4 .. 10 (HiRep's shift = -sigma): 22 systems, |r|/|b| < 1e-12
+B_DIMS, B_NG, B_MASS, B_CSW, B_EPS, B_SEED = (48, 24, 24, 24), 3, -0.3, 1.0, 0.3, 21
+
+
+def run_batch_solves(torch, stream, G, F):
+    """22 systems in one batched mixed-precision solve vs 22 sequential FP64 solves."""
+    lat = G.Lattice(*B_DIMS, B_NG, G.SYM)
+    u = F.smooth_gauge(B_SEED, lat.V, B_NG, B_EPS)
+    lat.set_gauge(u)
+    lat.represent_gauge_field(True)
+    lat.clover_init(B_CSW)
+    sig = np.logspace(-4, 1, 10)
+    shifts = [[0.0] + list(-sig)] + [[0.0] for _ in range(11)]
+    srcs = [lat.field(G.EVEN, host=F.point_source(lat.VH, lat.nf, spin=b, col=c)) for c in range(3) for b in range(4)]
+    xb = [lat.field(G.EVEN) for sh in shifts for _ in sh]
+    xs = [lat.field(G.EVEN) for sh in shifts for _ in sh]
+    op = G.OP_G5CPHI_EOPRE_SQ
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        r = fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b), r
+
+    out = {"workload": "SU(3) sym (NF=6), clover csw=1.0, m0=-0.3, 24^3x48, U=exp(i0.3H) seed 21; "
+                       "12 point sources + 10 shifts 1e-4..10 on source 0 = 22 systems",
+           "err2": ERR2}
+    # warm-up: kernel tuning and graph captures happen on first use
+    lat.cg_mshift_batch(op, B_MASS, srcs, shifts, ERR2, xb, flt=True)
+    ms, (its, ok) = timed(lambda: lat.cg_mshift_batch(op, B_MASS, srcs, shifts, ERR2, xb, flt=True))
+    out["batch_mixed_ms"], out["batch_mixed_ok"] = ms, bool(ok)
+    out["batch_mixed_iters_per_source"] = [int(i) for i in its]
+    lat.cg_mshift_batch(op, B_MASS, srcs, shifts, ERR2, xs, flt=False)
+    ms, (its, ok) = timed(lambda: lat.cg_mshift_batch(op, B_MASS, srcs, shifts, ERR2, xs, flt=False))
+    out["batch_fp64_ms"], out["batch_fp64_ok"] = ms, bool(ok)
+    # sequential FP64: HiRep's cg_mshift one system at a time (zero start)
+    tmp = lat.field(G.EVEN)
+    lat.g5Cphi_eopre_sq(B_MASS, tmp, srcs[0])  # tunes the single-field kernels
+
+    def sequential():
+        j, n_it, all_ok = 0, 0, True
+        for s, sh in enumerate(shifts):
+            for sg in sh:
+                lat.la("zero", xs[j])
+                it, ok = lat.cg_mshift(op, B_MASS, [sg], ERR2, srcs[s], [xs[j]])
+                n_it += it
+                all_ok = all_ok and ok
+                j += 1
+        return n_it, all_ok
+
+    ms, (n_it, ok) = timed(sequential)
+    out["sequential_fp64_ms"], out["sequential_fp64_ok"], out["sequential_fp64_mvm"] = ms, bool(ok), int(n_it)
+    # errors of the batched mixed solutions: against the sequential FP64 ones, and
+    # true residuals with the FP64 single-field operator
+    j, err, res = 0, 0.0, 0.0
+    for s, sh in enumerate(shifts):
+        for sg in sh:
+            lat.g5Cphi_eopre_sq(B_MASS, tmp, xb[j])
+            lat.la("mul_add_assign", tmp, -sg, xb[j])
+            lat.la("sub_assign", tmp, srcs[s])
+            res = max(res, float(np.sqrt(lat.sqnorm(tmp) / lat.sqnorm(srcs[s]))))
+            lat.la("copy", tmp, xb[j])
+            lat.la("sub_assign", tmp, xs[j])
+            err = max(err, float(np.sqrt(lat.sqnorm(tmp) / lat.sqnorm(xs[j]))))
+            j += 1
+    out["batch_mixed_max_true_rel_residual"] = res
+    out["batch_mixed_max_rel_error_vs_fp64"] = err
+    out["speedup_batch_mixed_vs_sequential_fp64"] = out["sequential_fp64_ms"] / out["batch_mixed_ms"]
+    out["speedup_batch_fp64_vs_sequential_fp64"] = out["sequential_fp64_ms"] / out["batch_fp64_ms"]
+    for q in (G.DOUBLE, G.FLOAT):
+        for ep in (1, 2):
+            ch, tms = G.ctypes.c_int(), (G.ctypes.c_float * 3)()
+            lat.L.hrgpu_batch_tuning(q, ep, 12, G.ctypes.byref(ch), tms)
+            out[f"tuning_{'f64' if q == G.DOUBLE else 'f32'}_ep{ep}_nb12"] = [ch.value] + [round(t, 4) for t in tms]
     return out
 
 
