@@ -182,6 +182,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 22-system solve (24^3x48 sextet)")
+    ap.add_argument("--batch-op", default=None, metavar="TxXxYxZ",
+                    help="only time the batched g5Cphi_eopre of the batched workload on this lattice")
+    ap.add_argument("--nb", type=int, default=12, help="fields per batch for --batch-op")
+    ap.add_argument("--prec", default="f", choices=["f", "d"], help="precision for --batch-op")
+    ap.add_argument("--batch-variant", type=int, default=-1, help="batch kernel variant (-1: autotune)")
     ap.add_argument("--hop-variant", type=int, default=-1, help="hopping-kernel variant (-1: autotune)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -197,6 +202,8 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    if args.batch_op:
+        return batch_op_main(args, torch, G, F)
     dist = None
     if world > 1:
         import datetime
@@ -358,6 +365,42 @@ def run_solves(lat, fin, torch, stream, G, dist):
 # origin (colours 0-2 x 4 spins), source 0 also for 10 shifts sigma log-spaced
 # 1e-4 .. 10 (HiRep's shift = -sigma): 22 systems, |r|/|b| < 1e-12
 B_DIMS, B_NG, B_MASS, B_CSW, B_EPS, B_SEED = (48, 24, 24, 24), 3, -0.3, 1.0, 0.3, 21
+
+
+def batch_op_main(args, torch, G, F):
+    """Time the batched g5Cphi_eopre alone (the batched workload's operator) on one lattice."""
+    T, X, Y, Z = (int(v) for v in args.batch_op.split("x"))
+    lat = G.Lattice(T, X, Y, Z, B_NG, G.SYM)
+    lat.set_gauge(F.smooth_gauge(B_SEED, lat.V, B_NG, B_EPS))
+    lat.represent_gauge_field(True)
+    lat.clover_init(B_CSW)
+    G._check(lat.L.hrgpu_set_batch_variant(args.batch_variant), "set_batch_variant")
+    prec = G.FLOAT if args.prec == "f" else G.DOUBLE
+    dt = np.complex64 if prec == G.FLOAT else np.complex128
+    fs = [lat.field(G.EVEN, prec, host=F.gaussian_spinor(i, lat.VH, lat.nf).astype(dt)) for i in range(args.nb)]
+    bi, bo = lat.batch(args.nb, prec, fields=fs), lat.batch(args.nb, prec)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        lat.apply_op_batch(G.OP_G5CPHI_EOPRE, B_MASS, bo, bi)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(args.steps):
+        lat.apply_op_batch(G.OP_G5CPHI_EOPRE, B_MASS, bo, bi)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    # bytes that must move per application: links and clover blocks once per hop,
+    # the fields in and out of each hop (and the aux read of the second)
+    esz = 8 if prec == G.FLOAT else 16
+    nf = lat.nf
+    links = 2 * lat.V * 4 * nf * nf * esz  # both hops read every link
+    clover = lat.V * 2 * (2 * nf * esz // 2 + nf * (2 * nf - 1) * esz)  # one packed block pair per site and hop
+    fields = args.nb * lat.VH * 4 * nf * esz * 5  # hop 1: in, out; hop 2: in, aux, out
+    nbytes = links + clover + fields
+    print(json.dumps({"batch_op": args.batch_op, "nb": args.nb, "prec": args.prec, "variant": args.batch_variant,
+                      "ms_per_application": ms, "ms_per_field": ms / args.nb, "bytes_per_application": nbytes,
+                      "GBps": nbytes / (ms * 1e-3) / 1e9}), flush=True)
 
 
 def run_batch_solves(torch, stream, G, F):
