@@ -182,6 +182,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 22-system solve (24^3x48 sextet)")
+    ap.add_argument("--no-force", action="store_true", help="skip the force check (16^4 SU(4) antisymmetric)")
     ap.add_argument("--batch-op", default=None, metavar="TxXxYxZ",
                     help="only time the batched g5Cphi_eopre of the batched workload on this lattice")
     ap.add_argument("--nb", type=int, default=12, help="fields per batch for --batch-op")
@@ -305,6 +306,8 @@ def main():
         line["solve"] = solve
     if world == 1 and not args.no_batch:
         line["solve_batch"] = run_batch_solves(torch, stream, G, F)
+    if world == 1 and not args.no_force:
+        line["force"] = run_force_check(torch, stream, G, F)
     if rank == 0 and world == 1 and not args.no_cpu:
         base, _ = cpu_reference_arm(args)
         line["cpu_baseline"] = base
@@ -365,6 +368,90 @@ def run_solves(lat, fin, torch, stream, G, dist):
 # origin (colours 0-2 x 4 spins), source 0 also for 10 shifts sigma log-spaced
 # 1e-4 .. 10 (HiRep's shift = -sigma): 22 systems, |r|/|b| < 1e-12
 B_DIMS, B_NG, B_MASS, B_CSW, B_EPS, B_SEED = (48, 24, 24, 24), 3, -0.3, 1.0, 0.3, 21
+
+
+# force workload: SU(4) two-index antisymmetric (NF = 6), Wilson m0 = -0.1, 16^4,
+# U = exp(i 0.25 H) seed 11, phi = D^+ eta (eta Gaussian, seed 11),
+# S = phi^+ (H^2)^-1 phi with H = g5 D_eopre
+F_DIMS, F_NG, F_MASS, F_EPS, F_SEED = (16, 16, 16, 16), 4, -0.1, 0.25, 11
+
+
+def run_force_check(torch, stream, G, F, ndir=4, step=1e-3):
+    """Pseudofermion force: kernel time, and its error against central differences of S
+    (fourth-order stencil) along ndir random su(4) directions on every link; FP64
+    solves to err2 = 1e-28.  S is about 8e5 here and a solve leaves it about 1e-8
+    uncertain, so the step is 1e-3 (truncation of the stencil ~ step^4 / 30).
+    Also the force from an X solved by the FP32-inner defect-correction CG,
+    against the FP64 force."""
+    lat = G.Lattice(*F_DIMS, F_NG, G.ASYM)
+    u0 = F.smooth_gauge(F_SEED, lat.V, F_NG, F_EPS)
+    lat.set_gauge(u0)
+    lat.represent_gauge_field(True)
+    nf, V, VH = lat.nf, lat.V, lat.VH
+    g5 = np.array([1, 1, -1, -1])[None, :, None]
+    eta = F.gaussian_spinor(F_SEED, VH, nf)
+    fe, tmp = lat.field(G.EVEN, host=g5 * eta), lat.field(G.EVEN)
+    lat.Dphi_eopre(F_MASS, tmp, fe)
+    phi = lat.field(G.EVEN, host=g5 * tmp.download())
+    x, y = lat.field(G.EVEN), lat.field(G.EVEN)
+    op = G.OP_G5DPHI_EOPRE_SQ
+    gT = lat.generators()
+
+    def solve(flt=False, err2=1e-28):
+        lat.la("zero", x)
+        _, ok = lat.cg_mshift(op, F_MASS, [0.0], err2, phi, [x], flt=flt)
+        assert ok
+        return lat.prod_re(phi, x)
+
+    def force():
+        lat.g5Dphi_eopre(F_MASS, y, x)
+        Xs = np.zeros((V, 4, nf), complex)
+        Ys = np.zeros_like(Xs)
+        Xs[:VH], Ys[:VH] = y.download(), x.download()
+        fX, fY = lat.field(G.FULL, host=Xs), lat.field(G.FULL, host=Ys)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        lat.fermion_force_begin()
+        a.record(stream)
+        lat.force_fermion_core(fX, fY, 1, 1.0, 1.0)
+        b.record(stream)
+        f = lat.fermion_force_end(1.0, np.zeros((V, 4, F_NG * F_NG - 1)))
+        return f, a.elapsed_time(b)
+
+    torch.cuda.synchronize()
+    t0 = time.time()
+    solve()
+    solve_s = time.time() - t0
+    f64, _ = force()
+    core_ms = float(np.median([force()[1] for _ in range(5)]))
+    solve(flt=True, err2=1e-26)
+    f32, _ = force()
+    rng = np.random.default_rng(32)
+    worst = 0.0
+    flat = u0.reshape(V * 4, F_NG, F_NG)
+    for _ in range(ndir):
+        w = rng.standard_normal((V * 4, F_NG * F_NG - 1))
+
+        def action(eps):
+            X = np.einsum("ka,aij->kij", eps * w, gT)
+            u = np.einsum("kij,kjl->kil", F.exp_i_hermitian(X), flat)
+            lat.set_gauge(u.reshape(V, 4, F_NG, F_NG))
+            lat.represent_gauge_field(True)
+            return solve()
+
+        s1 = action(step) - action(-step)
+        s2 = action(2 * step) - action(-2 * step)
+        fd = (8 * s1 - s2) / (12 * step)
+        an = float(-0.5 * np.sum(w * f64.reshape(V * 4, -1)))
+        worst = max(worst, abs(fd - an) / abs(an))
+    lat.set_gauge(u0)
+    lat.represent_gauge_field(True)
+    return {"workload": "SU(4) antisymmetric (NF=6), Wilson m0=-0.1, 16^4, U=exp(i0.25H) seed 11, "
+                        "phi = D^+ eta; S = phi^+ (H^2)^-1 phi",
+            "force_fermion_core_ms": core_ms, "fp64_solve_s": solve_s,
+            "fd": f"{ndir} random su(4) directions on all links, 4th-order central differences, step {step}",
+            "fd_max_rel_err_fp64": worst,
+            "mixed_vs_fp64_force_rel_err": float(np.abs(f32 - f64).max() / np.abs(f64).max())}
 
 
 def batch_op_main(args, torch, G, F):

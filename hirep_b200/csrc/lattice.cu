@@ -398,6 +398,13 @@ int hrgpu_finalize(void) {
 
 int hrgpu_nf(void) { return L.nf; }
 
+int hrgpu_algebra_generators(double *T) {
+  HR_REQUIRE(L.ready && L.h_gT, HRGPU_E_STATE, "algebra_generators: lattice not initialised");
+  HR_REQUIRE(T, HRGPU_E_ARG, "algebra_generators: NULL output");
+  memcpy(T, L.h_gT, sizeof(double) * 2 * (size_t)L.dimg * L.ng * L.ng);
+  return 0;
+}
+
 size_t hrgpu_spinor_bytes(int par, int prec) {
   if (!L.ready) return 0;
   return spinor_bytes(par, prec);

@@ -305,6 +305,12 @@ class Lattice:
         return it, True
 
     # force -------------------------------------------------------------------
+    def generators(self):
+        """T_A of su(NG) (Tr T_A T_B = delta/2), the basis of forces and momenta."""
+        t = np.empty((self.dimg, self.ng, self.ng), np.complex128)
+        _check(self.L.hrgpu_algebra_generators(_ptr(t)), "algebra_generators")
+        return t
+
     def fermion_force_begin(self):
         _check(self.L.hrgpu_fermion_force_begin(), "fermion_force_begin")
 

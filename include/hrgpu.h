@@ -72,6 +72,9 @@ int hrgpu_geometry(int T, int X, int Y, int Z, int *ipt, int *iup, int *idn);
 int hrgpu_finalize(void);
 const char *hrgpu_last_error(void);
 int hrgpu_nf(void);
+/* the basis T_A of su(NG) in which forces and momenta are expanded (autosun's
+ * generators, Tr T_A T_B = delta_AB / 2): T[A][i][j] complex, A < NG*NG-1 */
+int hrgpu_algebra_generators(double *T);
 /* bytes of one device spinor field of the given parity and precision */
 size_t hrgpu_spinor_bytes(int par, int prec);
 /* all work is issued on this stream; NULL is the legacy default stream (stream 0).

@@ -199,3 +199,13 @@ def test_gpu_force_mixed_precision_solve():
     f32 = model32.force()
     err = np.abs(f32 - f64).max() / np.abs(f64).max()
     assert err < 1e-9, err
+
+
+@pytest.mark.gpu
+def test_library_generators_are_the_oracle_basis():
+    from hirep_b200 import hrgpu as G
+
+    for ng, rep in ((2, O.ADJ), (3, O.FUND), (4, O.ASYM)):
+        o = O.Oracle(4, 4, 4, 4, ng, rep)
+        lat = G.Lattice(4, 4, 4, 4, ng, {O.FUND: G.FUND, O.ADJ: G.ADJ, O.ASYM: G.ASYM}[rep], ipt=o.geometry()[0])
+        assert np.abs(lat.generators() - o.generators()[0]).max() < 1e-15
