@@ -198,6 +198,7 @@ def main():
 
     from hirep_b200 import fields as F
     from hirep_b200 import hrgpu as G
+    from hirep_b200.replicas import max_over_ranks, replica_rate
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -253,12 +254,8 @@ def main():
         clk.t1 = time.time()
     launches = 2 * args.steps
     step_ms = sum(a.elapsed_time(b) for a, b in evs) / args.steps
-    t_max = step_ms
-    if dist:
-        tt = torch.tensor([step_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-    value = world * nbytes / (t_max * 1e-3) / 1e9
+    t_max = max_over_ranks(step_ms, dist, "cuda")
+    value = replica_rate(nbytes, t_max, world) / 1e9
 
     # end to end through the C ABI: host (pinned) -> device, operator, device -> host
     h_in = torch.from_numpy(src.view(np.float64)).pin_memory()
@@ -276,11 +273,7 @@ def main():
         torch.cuda.synchronize()
         if k >= args.warmup:
             e2e.append(a.elapsed_time(b))
-    e2e_ms = float(np.mean(e2e))
-    if dist:
-        tt = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
+    e2e_ms = max_over_ranks(float(np.mean(e2e)), dist, "cuda")
 
     solve = None
     if not args.no_solve:
@@ -296,7 +289,7 @@ def main():
                      "frac": nbytes / (t_max * 1e-3) / 1e9 / peak, "peak_kind": peak_kind,
                      "kernel": "k_hop (2 launches per Cphi_eopre)", "algorithmic_bytes_per_step": nbytes,
                      "traffic": profile_traffic()},
-        "e2e": {"value": world * nbytes / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "ms_per_step": e2e_ms,
+        "e2e": {"value": replica_rate(nbytes, e2e_ms, world) / 1e9, "unit": "GB/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "hop_tuning": hop_tuning(lat, G),
