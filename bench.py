@@ -345,7 +345,29 @@ def run_solves(lat, fin, torch, stream, G, dist):
             iters = it
         out[name + "_ms"] = float(np.median(times))
         out[name + "_mvm"] = iters
+    # the same mixed solve with the FP32 operator reading BF16 links
+    x16 = lat.field(G.EVEN)
+    G._check(lat.L.hrgpu_set_flt_link_storage(G.LINKS_BF16), "set_flt_link_storage")
+    try:
+        times = []
+        for rep in range(3):
+            lat.la("zero", x16)
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            it, ok = lat.cg_mshift(G.OP_G5CPHI_EOPRE_SQ, MASS, [0.0], ERR2, fin, [x16], flt=True)
+            b.record(stream)
+            torch.cuda.synchronize()
+            if rep > 0:
+                times.append(a.elapsed_time(b))
+        out["mixed_bf16_links_ms"], out["mixed_bf16_links_mvm"], out["mixed_bf16_links_ok"] = (
+            float(np.median(times)), it, bool(ok))
+    finally:
+        G._check(lat.L.hrgpu_set_flt_link_storage(G.LINKS_F32), "set_flt_link_storage")
     r = lat.field(G.EVEN)
+    lat.g5Cphi_eopre_sq(MASS, r, x16)
+    lat.la("sub_assign", r, fin)
+    out["mixed_bf16_links_true_rel_residual"] = float(np.sqrt(lat.sqnorm(r) / lat.sqnorm(fin)))
     lat.g5Cphi_eopre_sq(MASS, r, x32)
     lat.la("sub_assign", r, fin)
     out["mixed_true_rel_residual"] = float(np.sqrt(lat.sqnorm(r) / lat.sqnorm(fin)))

@@ -21,7 +21,8 @@ static double g_static_mass = 0.0;
 
 template <typename R>
 static const void *links() {
-  return sizeof(R) == 8 ? L.U : L.Uf;
+  if (sizeof(R) == 8) return L.U;
+  return L.flt_links == HRGPU_LINKS_BF16 ? L.Ubf : L.Uf;
 }
 
 // one hop onto parity outp with the given epilogue; fields are parity fields
@@ -41,6 +42,10 @@ int hop(int outp, void *out, const void *in, int ep, double cacc, const void *au
   a.outp = outp;
   a.g5 = g5;
   a.stop = L.cur_stop;
+  if (sizeof(R) == 4 && L.flt_links == HRGPU_LINKS_BF16) {
+    if (int rc = ensure_links_bf16()) return rc;
+    a.U = L.Ubf;
+  }
   g_mvm++;
   return launch_hop<R>(ep, a);
 }
@@ -229,7 +234,7 @@ int hrgpu_set_hop_variant(int variant) {
 }
 
 int hrgpu_hop_tuning(int prec, int epilogue, int *chosen, float *ms) {
-  HR_REQUIRE(prec >= 0 && prec <= 1 && epilogue >= 0 && epilogue <= 2 && chosen && ms, HRGPU_E_ARG,
+  HR_REQUIRE(prec >= 0 && prec <= 2 && epilogue >= 0 && epilogue <= 2 && chosen && ms, HRGPU_E_ARG,
              "hop_tuning: bad arguments");
   *chosen = L.hop_variant[prec][epilogue];
   for (int v = 0; v < HOP_VARIANTS; v++) ms[v] = L.hop_tune_ms[prec][epilogue][v];
@@ -250,6 +255,13 @@ int hrgpu_g5Cphi_eopre(double mass, void *out, const void *in) { return Cphi_eo<
 int hrgpu_g5Cphi_eopre_sq(double mass, void *out, const void *in) { return sq<double>(op_ceo_d, mass, out, in, HRGPU_EVEN); }
 int hrgpu_g5Cphi_eopre_flt(double mass, void *out, const void *in) { return Cphi_eo<float>(mass, out, in, 1, nullptr); }
 int hrgpu_g5Cphi_eopre_sq_flt(double mass, void *out, const void *in) { return sq<float>(op_ceo_f, mass, out, in, HRGPU_EVEN); }
+
+int hrgpu_set_flt_link_storage(int kind) {
+  HR_REQUIRE(kind == HRGPU_LINKS_F32 || kind == HRGPU_LINKS_BF16, HRGPU_E_ARG,
+             "set_flt_link_storage: kind must be HRGPU_LINKS_F32 or HRGPU_LINKS_BF16");
+  L.flt_links = kind;
+  return 0;
+}
 
 int hrgpu_set_dirac_mass(double mass) {
   g_static_mass = mass;

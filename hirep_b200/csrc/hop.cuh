@@ -14,6 +14,8 @@
 //   EP_CLOV      out = cacc*acc + Hdiag*aux         (Cphi, Cphi_eopre second hop)
 // then optionally gamma_5, and optionally a per-block partial of |out|^2.
 #pragma once
+#include <cuda_bf16.h>
+
 #include <type_traits>
 
 #include "hrgpu_internal.cuh"
@@ -93,6 +95,56 @@ __device__ __forceinline__ void link_mul(V *chi, const V *h, const R *U, long pl
   }
 }
 
+// links stored in BF16 (the FP32 operator's optional storage): the products are FP32
+template <int NA, bool DAG>
+__device__ __forceinline__ void link_mul(float2 *chi, const float2 *h, const __nv_bfloat162 *U, long plane, long site,
+                                         int nf) {
+#pragma unroll
+  for (int i = 0; i < NA; i++) {
+    if (i >= nf) break;
+    float2 a = make_float2(0.f, 0.f);
+#pragma unroll (Unroll<NA>::v)
+    for (int j = 0; j < NA; j++) {
+      if (j >= nf) break;
+      if (!DAG) {
+        float2 u = __bfloat1622float2(__ldg(U + (long)(i * nf + j) * plane + site));
+        cmac(a, u, h[j]);
+      } else {
+        float2 u = __bfloat1622float2(__ldg(U + (long)(j * nf + i) * plane + site));
+        cmacc(a, u, h[j]);
+      }
+    }
+    chi[i] = a;
+  }
+}
+
+template <int NA, bool DAG>
+__device__ __forceinline__ void link_mul(float2 *chi, const float2 *h, const __nv_bfloat16 *U, long plane, long site,
+                                         int nf) {
+#pragma unroll
+  for (int i = 0; i < NA; i++) {
+    if (i >= nf) break;
+    float2 a = make_float2(0.f, 0.f);
+#pragma unroll (Unroll<NA>::v)
+    for (int j = 0; j < NA; j++) {
+      if (j >= nf) break;
+      float u = __bfloat162float(DAG ? __ldg(U + (long)(j * nf + i) * plane + site) : __ldg(U + (long)(i * nf + j) * plane + site));
+      rmac(a, u, h[j]);
+    }
+    chi[i] = a;
+  }
+}
+
+// BF16 storage type of a link element
+template <bool REAL>
+struct LinkBF16 {
+  typedef __nv_bfloat162 T;
+};
+template <>
+struct LinkBF16<true> {
+  typedef __nv_bfloat16 T;
+};
+
 // y = H x for one packed Hermitian 2NF x 2NF block (diag real, strict lower complex)
 template <int NA, typename V, typename R>
 __device__ __forceinline__ void herm_apply(V *y, const V *x, const R *dg, const V *od, long plane, long site, int nf) {
@@ -169,10 +221,11 @@ __device__ __forceinline__ void clover_epilogue(V (&ra)[NA], V (&rb)[NA], const 
 }
 
 // one output site (checkerboard index cb < VH) of the hop; returns |out|^2 when a.red is set
-template <int NFT, bool REAL, typename R, int EP>
+// LE: the storage type of a link element (BF16 for the FP32 operator's optional link copy)
+template <int NFT, bool REAL, typename R, int EP, typename LE = typename LinkE<REAL, R>::T>
 __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb) {
   typedef typename C2<R>::T V;
-  typedef typename LinkE<REAL, R>::T E;
+  typedef LE E;
   constexpr int NA = NFT;
   const int nf = NFT;
   const Geo g = a.g;
@@ -295,12 +348,12 @@ __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb) {
   return nrm;
 }
 
-template <int NFT, bool REAL, typename R, int EP, int MINB>
+template <int NFT, bool REAL, typename R, int EP, int MINB, typename LE = typename LinkE<REAL, R>::T>
 __global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop(HopArgs<R> a) {
   if (a.stop && *a.stop) return;
   const int cb = blockIdx.x * blockDim.x + threadIdx.x;
   double nrm = 0.0;
-  if (cb < a.g.VH) nrm = hop_site<NFT, REAL, R, EP>(a, cb);
+  if (cb < a.g.VH) nrm = hop_site<NFT, REAL, R, EP, LE>(a, cb);
   if (a.red) block_partial<R>(nrm, a.red);
 }
 
@@ -337,10 +390,10 @@ __device__ __forceinline__ V mul_unit(V v, int re, int im) {
 
 // one thread (half h of the pair) of site cb; inactive threads compute but do
 // not write (their partner needs the shuffles)
-template <int NFT, bool REAL, typename R, int EP>
+template <int NFT, bool REAL, typename R, int EP, typename LE = typename LinkE<REAL, R>::T>
 __device__ __forceinline__ double hop2_site(const HopArgs<R> &a, const int cb, const int h, const bool active) {
   typedef typename C2<R>::T V;
-  typedef typename LinkE<REAL, R>::T E;
+  typedef LE E;
   constexpr int NA = NFT;
   const int nf = NFT;
   const Geo g = a.g;
@@ -461,13 +514,13 @@ __device__ __forceinline__ double hop2_site(const HopArgs<R> &a, const int cb, c
   return active ? nrm : 0.0;
 }
 
-template <int NFT, bool REAL, typename R, int EP, int MINB>
+template <int NFT, bool REAL, typename R, int EP, int MINB, typename LE = typename LinkE<REAL, R>::T>
 __global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop2(HopArgs<R> a) {
   if (a.stop && *a.stop) return;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = (tid >> 1) < a.g.VH;
   const int cb = active ? (tid >> 1) : a.g.VH - 1;
-  double nrm = hop2_site<NFT, REAL, R, EP>(a, cb, tid & 1, active);
+  double nrm = hop2_site<NFT, REAL, R, EP, LE>(a, cb, tid & 1, active);
   if (a.red) block_partial<R>(nrm, a.red);
 }
 

@@ -47,6 +47,35 @@ int launch_ep_variant(HopArgs<R> &a, int variant) {
     break;
 #define HOPC(N) HOPV(N, false)
 #define HOPR(N) HOPV(N, true)
+  // FP32 operator with BF16 link storage: variants 0-3 (no cp.async form)
+#define HOPVB(N, RL)                                                                            \
+  case N:                                                                                       \
+    switch (variant) {                                                                          \
+      case 0: k_hop<N, RL, float, EP, 1, typename LinkBF16<RL>::T><<<grid, block, 0, s>>>(a); break;  \
+      case 1: k_hop2<N, RL, float, EP, 1, typename LinkBF16<RL>::T><<<grid, block, 0, s>>>(a); break; \
+      case 2: k_hop<N, RL, float, EP, 4, typename LinkBF16<RL>::T><<<grid, block, 0, s>>>(a); break;  \
+      case 3: k_hop2<N, RL, float, EP, 4, typename LinkBF16<RL>::T><<<grid, block, 0, s>>>(a); break; \
+      default: return -1;                                                                       \
+    }                                                                                           \
+    break;
+  if constexpr (std::is_same<R, float>::value) {
+    if (L.flt_links == HRGPU_LINKS_BF16) {
+      if (!L.real) {
+        switch (L.nf) {
+          HOPVB(2, false) HOPVB(3, false) HOPVB(4, false) HOPVB(5, false) HOPVB(6, false) HOPVB(10, false)
+          default: set_error("no hopping kernel instantiated for complex NF=%d", L.nf); return HRGPU_E_NF;
+        }
+      } else {
+        switch (L.nf) {
+          HOPVB(3, true) HOPVB(8, true) HOPVB(15, true)
+          default: set_error("no hopping kernel instantiated for real NF=%d", L.nf); return HRGPU_E_NF;
+        }
+      }
+      HR_LAUNCH_CHECK();
+      return 0;
+    }
+  }
+#undef HOPVB
   if (!L.real) {
     switch (L.nf) {
       HOPC(2) HOPC(3) HOPC(4) HOPC(5) HOPC(6) HOPC(10)
@@ -72,7 +101,8 @@ int launch_ep_variant(HopArgs<R> &a, int variant) {
 // a variant (tests use it to check both).
 template <typename R, int EP>
 int launch_ep(HopArgs<R> &a) {
-  const int pi = sizeof(R) == 8 ? 0 : 1;
+  // tuning slots: FP64, FP32, FP32 with BF16 links
+  const int pi = sizeof(R) == 8 ? 0 : (L.flt_links == HRGPU_LINKS_BF16 ? 2 : 1);
   int &v = L.hop_variant[pi][EP];
   if (L.hop_force >= 0) {
     int rc = launch_ep_variant<R, EP>(a, L.hop_force);

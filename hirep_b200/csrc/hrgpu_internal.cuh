@@ -95,9 +95,14 @@ struct Lattice {
   double *h_partials = nullptr;   // pinned host mirror of the final values
   double *d_scalars = nullptr;    // CG scalars
   const int *cur_stop = nullptr;  // set by the inverters while they drive the operator
-  int hop_variant[2][3] = {{-1, -1, -1}, {-1, -1, -1}};  // tuned hopping-kernel variant [prec][epilogue]
+  // tuned hopping-kernel variant [FP64, FP32, FP32 with BF16 links][epilogue]
+  int hop_variant[3][3] = {{-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}};
   int hop_force = -1;             // forced variant (-1: autotune)
-  float hop_tune_ms[2][3][HOP_VARIANTS] = {};  // tuning times of the variants [prec][epilogue][variant]
+  float hop_tune_ms[3][3][HOP_VARIANTS] = {};  // tuning times of the variants [slot][epilogue][variant]
+  // storage of the links read by the FP32 operators: HRGPU_LINKS_F32 (Uf) or HRGPU_LINKS_BF16 (Ubf)
+  int flt_links = 0;
+  void *Ubf = nullptr;
+  unsigned long ubf_gen = ~0UL;
   // multi-field kernel: tuned variant + 1 (0 = not tuned yet) [prec][epilogue][nb], its timings, forced variant
   signed char hopb_variant[2][3][HOPB_MAXNB + 1] = {};
   float hopb_tune_ms[2][3][HOPB_MAXNB + 1][HOPB_VARIANTS] = {};
@@ -121,6 +126,7 @@ inline size_t spinor_bytes(int par, int prec) {
 }
 
 int ensure_tmp(void **p, size_t bytes);
+int ensure_links_bf16();  // the BF16 copy of the links, made from the FP64 ones when they changed
 int compute_clover_term_dev();
 void cg_release();
 int ensure_stage(size_t bytes);

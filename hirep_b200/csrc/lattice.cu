@@ -6,6 +6,8 @@
 #include <complex>
 #include <vector>
 
+#include <cuda_bf16.h>
+
 #include "hrgpu_internal.cuh"
 
 namespace hrgpu {
@@ -61,7 +63,7 @@ static void free_ptr(void *p) {
 
 static void free_all() {
   cg_release();
-  void *ptrs[] = {L.d_h2d, L.d_d2h, L.U, L.Uf, L.Ug, L.cl_term, L.cl_dg, L.cl_od, L.cl_idg, L.cl_iod,
+  void *ptrs[] = {L.d_h2d, L.d_d2h, L.U, L.Uf, L.Ubf, L.Ug, L.cl_term, L.cl_dg, L.cl_od, L.cl_idg, L.cl_iod,
                   L.cl_dg_f, L.cl_idg_f, L.cl_od_f, L.cl_iod_f, L.force_sum, L.cl_force, L.d_proj_off,
                   L.d_proj_k, L.d_proj_c, L.partials, L.d_scalars, L.tmp_o, L.tmp_e, L.tmp_e2, L.tmp_full,
                   L.tmp_full2, L.tmp_o_f, L.tmp_e_f, L.tmp_full_f, L.stage};
@@ -549,6 +551,32 @@ int hrgpu_gauge_get_f(void *uf_host) {
   HR_REQUIRE(L.ready && L.have_gauge, HRGPU_E_STATE, "hrgpu_gauge_get_f: no gauge field");
   return links_out(uf_host, L.U, L.nf * L.nf, L.real ? 8 : 16, 4);
 }
+
+}  // extern "C"
+
+namespace hrgpu {
+
+__global__ void k_links_bf16(void *dst, const double *src, long n, int real) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    if (real) ((__nv_bfloat16 *)dst)[i] = __double2bfloat16(src[i]);
+    else ((__nv_bfloat162 *)dst)[i] = __halves2bfloat162(__double2bfloat16(src[2 * i]), __double2bfloat16(src[2 * i + 1]));
+  }
+}
+
+int ensure_links_bf16() {
+  HR_REQUIRE(L.have_gauge, HRGPU_E_STATE, "no gauge field set");
+  if (L.Ubf && L.ubf_gen == L.gauge_gen) return 0;
+  const long n = (long)4 * L.nf * L.nf * 2 * L.ld;  // link elements (complex or real)
+  if (!L.Ubf) HR_CUDA(cudaMalloc(&L.Ubf, n * (L.real ? sizeof(__nv_bfloat16) : sizeof(__nv_bfloat162))));
+  k_links_bf16<<<nblk(n), 256, 0, L.stream>>>(L.Ubf, (const double *)L.U, n, L.real);
+  HR_LAUNCH_CHECK();
+  L.ubf_gen = L.gauge_gen;
+  return 0;
+}
+
+}  // namespace hrgpu
+
+extern "C" {
 
 int hrgpu_assign_ud2u_f(void) {
   HR_REQUIRE(L.ready && L.have_gauge, HRGPU_E_STATE, "hrgpu_assign_ud2u_f: no gauge field");

@@ -138,10 +138,20 @@ int hrgpu_g5Dphi_eopre_sq_flt(double m0, void *out, const void *in);
  * 4 = one thread per site with cp.async-pipelined loads (NF <= 4 complex, NF = 3
  * real), -1 = autotune on first use (default).  hrgpu_hop_tuning reports the
  * variant chosen for (precision, epilogue 0..2) and the per-launch times it
- * measured (ms has room for 5 values; -1 marks a variant not built for this NF).
+ * measured (ms has room for 5 values; -1 marks a variant not built for this NF);
+ * precision 2 is the FP32 operator reading BF16 links.
  * Tuning controls of this library; they have no counterpart in the reference. */
 int hrgpu_set_hop_variant(int variant);
 int hrgpu_hop_tuning(int prec, int epilogue, int *chosen, float *ms);
+/* Storage of the links read by the FP32 operators (the _flt operators, the
+ * inner solves of cg_mshift_flt): HRGPU_LINKS_F32 (default, assign_ud2u_f's
+ * copy) or HRGPU_LINKS_BF16 (a BF16 copy rounded from the FP64 links, FP32
+ * arithmetic).  BF16 halves the link bytes of the FP32 operator and makes its
+ * result differ from the FP32 one at the 1e-3 level; the FP64 defect
+ * correction of cg_mshift_flt still reaches the FP64 tolerance.  An experiment
+ * of this library, not in the reference. */
+enum { HRGPU_LINKS_F32 = 0, HRGPU_LINKS_BF16 = 1 };
+int hrgpu_set_flt_link_storage(int kind);
 /* getMVM (Dphi.c:105-113): hopping applications / 2 since the last call */
 unsigned long hrgpu_getMVM(void);
 
