@@ -184,6 +184,12 @@ int apply_op(int op, int prec, double mass, void *out, const void *in) {
       case HRGPU_OP_G5DPHI_EOPRE_SQ: return sq<double>(op_eo_d, mass, out, in, HRGPU_EVEN);
       case HRGPU_OP_G5CPHI_EOPRE_SQ: return sq<double>(op_ceo_d, mass, out, in, HRGPU_EVEN);
       case HRGPU_OP_G5CPHI_SQ: return sq<double>(op_cfull_d, mass, out, in, HRGPU_FULL);
+      case HRGPU_OP_DPHI_EOPRE: return op_eo_d(mass, out, in, 0);
+      case HRGPU_OP_G5DPHI_EOPRE: return op_eo_d(mass, out, in, 1);
+      case HRGPU_OP_CPHI_EOPRE: return op_ceo_d(mass, out, in, 0);
+      case HRGPU_OP_G5CPHI_EOPRE: return op_ceo_d(mass, out, in, 1);
+      case HRGPU_OP_DPHI: return op_Dfull_d(mass, out, in, 0);
+      case HRGPU_OP_CPHI: return op_cfull_d(mass, out, in, 0);
     }
   } else {
     switch (op) {
@@ -197,7 +203,11 @@ int apply_op(int op, int prec, double mass, void *out, const void *in) {
   return HRGPU_E_ARG;
 }
 
-int op_parity(int op) { return (op == HRGPU_OP_G5DPHI_SQ || op == HRGPU_OP_G5CPHI_SQ) ? HRGPU_FULL : HRGPU_EVEN; }
+int op_parity(int op) {
+  return (op == HRGPU_OP_G5DPHI_SQ || op == HRGPU_OP_G5CPHI_SQ || op == HRGPU_OP_DPHI || op == HRGPU_OP_CPHI)
+             ? HRGPU_FULL
+             : HRGPU_EVEN;
+}
 
 double static_mass() { return g_static_mass; }
 

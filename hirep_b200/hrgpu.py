@@ -18,7 +18,7 @@ EVEN, ODD, FULL = 0, 1, 2
 DOUBLE, FLOAT = 0, 1
 FUND, ADJ, SYM, ASYM = 0, 1, 2, 3
 OP_G5DPHI_SQ, OP_G5DPHI_EOPRE_SQ, OP_G5CPHI_EOPRE_SQ, OP_G5CPHI_SQ = 0, 1, 2, 3
-OP_DPHI_EOPRE, OP_G5DPHI_EOPRE, OP_CPHI_EOPRE, OP_G5CPHI_EOPRE = 4, 5, 6, 7
+OP_DPHI_EOPRE, OP_G5DPHI_EOPRE, OP_CPHI_EOPRE, OP_G5CPHI_EOPRE, OP_DPHI, OP_CPHI = 4, 5, 6, 7, 8, 9
 E_NOCONV = 5
 LINKS_F32, LINKS_BF16 = 0, 1
 
@@ -40,6 +40,7 @@ def lib():
         L.hrgpu_getMVM.restype = ctypes.c_ulong
         L.hrgpu_get_dirac_mass.restype = ctypes.c_double
         L.hrgpu_batch_bytes.restype = ctypes.c_size_t
+        L.hrgpu_mre_init.restype = ctypes.c_void_p
         _lib = L
     return _lib
 
@@ -115,6 +116,24 @@ class Batch:
         assert len(fields) == self.nb
         arr = (ctypes.c_void_p * self.nb)(*[f.ptr.value for f in fields])
         _check(lib().hrgpu_batch_unpack(arr, self.ptr, self.nb, self.prec), "batch_unpack")
+
+
+class MREHandle:
+    """Past solutions for the chronological initial guess (mre_store / mre_guess)."""
+
+    def __init__(self, lat, h):
+        self.lat, self.h = lat, h
+
+    def store(self, p, field):
+        _check(self.lat.L.hrgpu_mre_store(self.h, p, field.ptr), "mre_store")
+
+    def guess(self, p, out, op, mass, pf):
+        _check(self.lat.L.hrgpu_mre_guess(self.h, p, out.ptr, op, D(mass), pf.ptr), "mre_guess")
+
+    def free(self):
+        if self.h:
+            _check(self.lat.L.hrgpu_mre_free(self.h), "mre_free")
+            self.h = None
 
 
 class Lattice:
@@ -277,6 +296,33 @@ class Lattice:
             return it.value, False
         _check(rc, "cg_mshift_flt" if flt else "cg_mshift")
         return it.value, True
+
+    def g5QMR_mshift(self, op, mass, shifts, err2, inp, outs, max_iter=0):
+        n = len(shifts)
+        sh = np.ascontiguousarray(shifts, np.float64)
+        arr = (ctypes.c_void_p * n)(*[o.ptr.value for o in outs])
+        it = ctypes.c_int(0)
+        rc = self.L.hrgpu_g5QMR_mshift(op, D(mass), n, _ptr(sh), D(err2), max_iter, inp.ptr, arr, ctypes.byref(it))
+        if rc == E_NOCONV:
+            return it.value, False
+        _check(rc, "g5QMR_mshift")
+        return it.value, True
+
+    def MINRES(self, op, mass, err2, inp, out, trial=None, max_iter=0):
+        it = ctypes.c_int(0)
+        rc = self.L.hrgpu_MINRES(op, D(mass), D(err2), max_iter, inp.ptr, out.ptr,
+                                 None if trial is None else trial.ptr, ctypes.byref(it))
+        if rc == E_NOCONV:
+            return it.value, False
+        _check(rc, "MINRES")
+        return it.value, True
+
+    def mre(self, max_, par):
+        """An MRE handle (LibHR/Update/mre.c) for fields of parity par."""
+        h = self.L.hrgpu_mre_init(max_, par)
+        if not h:
+            raise HRGPUError("mre_init: " + self.L.hrgpu_last_error().decode())
+        return MREHandle(self, ctypes.c_void_p(h))
 
     # many right-hand sides -------------------------------------------------------
     def batch(self, nb, prec=DOUBLE, fields=None):

@@ -41,11 +41,13 @@ enum {
   HRGPU_OP_G5DPHI_EOPRE_SQ = 1, /* g5Dphi_eopre_sq(mass)  Dphi.c:988-998, even sites       */
   HRGPU_OP_G5CPHI_EOPRE_SQ = 2, /* g5Cphi_eopre_sq(mass)  Dphi.c:1263-1272, even sites     */
   HRGPU_OP_G5CPHI_SQ = 3,       /* g5Cphi_sq(mass)        Dphi.c:1226-1235, full lattice   */
-  /* not positive: hrgpu_apply_op_batch only */
+  /* not positive (the g5QMR / MINRES operators; eopre ones also for hrgpu_apply_op_batch) */
   HRGPU_OP_DPHI_EOPRE = 4,      /* Dphi_eopre(mass)       Dphi.c:874-907                   */
   HRGPU_OP_G5DPHI_EOPRE = 5,    /* g5Dphi_eopre(mass)     Dphi.c:950-985                   */
   HRGPU_OP_CPHI_EOPRE = 6,      /* Cphi_eopre(mass)       Dphi.c:1240-1255                 */
-  HRGPU_OP_G5CPHI_EOPRE = 7     /* g5Cphi_eopre(mass)     Dphi.c:1257-1261                 */
+  HRGPU_OP_G5CPHI_EOPRE = 7,    /* g5Cphi_eopre(mass)     Dphi.c:1257-1261                 */
+  HRGPU_OP_DPHI = 8,            /* Dphi(mass)             Dphi.c:703-783, full lattice     */
+  HRGPU_OP_CPHI = 9             /* Cphi(mass)             Dphi.c:1215-1221, full lattice   */
 };
 /* status codes */
 enum {
@@ -232,6 +234,28 @@ int hrgpu_cg_mshift(int op, double mass, int n, const double *shift, double err2
  * around an FP32 multi-shift CG on the float twin of op (clover included). */
 int hrgpu_cg_mshift_flt(int op, double mass, int n, const double *shift, double err2, int max_iter,
                         const void *in, void *const *out, int *iters);
+
+/* g5QMR_mshift (LibHR/Inverters/g5QMR_mshift.c:481-542) for the gamma_5-hermitian
+ * Dirac operator D (op: HRGPU_OP_DPHI_EOPRE, _CPHI_EOPRE, _DPHI, _CPHI):
+ * out[i] = (D - shift[i])^-1 in; with n == 1 out[0] is the initial guess.
+ * Unconverged shifts are solved again alone, then by MINRES on g5 (D - shift)
+ * as in the reference.  *iters gets the MVM count as HiRep counts it. */
+int hrgpu_g5QMR_mshift(int op, double mass, int n, const double *shift, double err2, int max_iter,
+                       const void *in, void *const *out, int *iters);
+/* MINRES (LibHR/Inverters/MINRES.c:160-172) for a hermitian op (g5Dphi_eopre,
+ * g5Cphi_eopre and the squared operators); trial may be NULL (start from zero). */
+int hrgpu_MINRES(int op, double mass, double err2, int max_iter, const void *in, void *out, const void *trial,
+                 int *iters);
+/* chronological initial guess, MRE (LibHR/Update/mre.c): a handle keeps the
+ * last max (<= 15) solutions of two sequences p = 0, 1 of fields of parity par.
+ * mre_guess builds the guess from them for DD = op (mre.c:230-268), keeping the
+ * reference's convention (the coefficients solve A x = conj(b) with
+ * A[j][i] = <DD v_i, v_j>, b_i = <v_i, pf>); a singular system gives out = 0.
+ * hrgpu_mre_init returns NULL on error (message in hrgpu_last_error). */
+void *hrgpu_mre_init(int max, int par);
+int hrgpu_mre_store(void *mre, int p, const void *in);
+int hrgpu_mre_guess(void *mre, int p, void *out, int op, double mass, const void *pf);
+int hrgpu_mre_free(void *mre);
 
 /* ------------------------------------------------------ batched (multi-RHS) -- */
 /* HiRep has no batched interface; these entry points serve its callers that

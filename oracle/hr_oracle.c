@@ -1241,7 +1241,10 @@ void orc_Cphi_diag_inv(double mass, cplx *out, const cplx *in, int par) { orc_Cp
 /* ------------------------------------------------------------------------- */
 /* multi-shift CG: LibHR/Inverters/cg_mshift.c:24-195                         */
 /* ------------------------------------------------------------------------- */
-static int op_sites(int op) { return (op == ORC_OP_G5DPHI_SQ || op == ORC_OP_G5CPHI_SQ) ? V_ : VH_; }
+static int op_sites(int op)
+{
+  return (op == ORC_OP_G5DPHI_SQ || op == ORC_OP_G5CPHI_SQ || op == ORC_OP_DPHI || op == ORC_OP_CPHI) ? V_ : VH_;
+}
 
 static void apply_op(int op, cplx *out, const cplx *in)
 {
@@ -1251,6 +1254,12 @@ static void apply_op(int op, cplx *out, const cplx *in)
   case ORC_OP_G5DPHI_EOPRE_SQ: orc_g5Dphi_eopre_sq(static_mass_, out, in); break;
   case ORC_OP_G5CPHI_EOPRE_SQ: orc_g5Cphi_eopre_sq(static_mass_, out, in); break;
   case ORC_OP_G5CPHI_SQ: orc_g5Cphi_sq(static_mass_, out, in); break;
+  case ORC_OP_DPHI_EOPRE: orc_Dphi_eopre(static_mass_, out, in); break;
+  case ORC_OP_G5DPHI_EOPRE: orc_g5Dphi_eopre(static_mass_, out, in); break;
+  case ORC_OP_CPHI_EOPRE: orc_Cphi_eopre(static_mass_, out, in); break;
+  case ORC_OP_G5CPHI_EOPRE: orc_g5Cphi_eopre(static_mass_, out, in); break;
+  case ORC_OP_DPHI: orc_Dphi(static_mass_, out, in); break;
+  case ORC_OP_CPHI: orc_Cphi(static_mass_, out, in); break;
   }
 }
 
@@ -1495,6 +1504,329 @@ int orc_cg_mshift_flt(int op, int n, const double *shift, double err2, int max_i
   free(res_flt);
   free(res);
   return siter + diter;
+}
+
+/* ------------------------------------------------------------------------- */
+/* g5QMR for gamma_5-hermitian operators: LibHR/Inverters/g5QMR_mshift.c      */
+/* ------------------------------------------------------------------------- */
+static double g5_prod_re_n(int ns, const cplx *a, const cplx *b) { return orc_g5_prod_re(ns, a, b); }
+
+/* plane rotation (c, s) with [c s; -s c] (a, b)^T = (1/r, 0)^T   (g5QMR_mshift.c:30-37) */
+static void givens(double *r, double *c, double *s, double a, double b)
+{
+  if (fabs(a) < 1.e-15)
+  {
+    *r = 1. / b;
+    *c = 0.;
+    *s = 1.;
+  }
+  else
+  {
+    double t = b / a;
+    *c = 1. / sqrt(1. + t * t);
+    *s = t * (*c);
+    *r = 1. / ((*c) * a + (*s) * b);
+  }
+}
+
+/* g5QMR_mshift_core (g5QMR_mshift.c:83-279): valid[i] = 1 if |M x_i - shift_i x_i - in|^2 <= err2 |in|^2.
+ * Returns the MVM count, or -1 when the gamma_5 norm of the start vector vanishes (HiRep stops there). */
+static int g5qmr_core(short *valid, int op, int n, const double *shift, double err2, int max_iter, const cplx *in,
+                      cplx *out)
+{
+  const int ns = op_sites(op);
+  const size_t fsz = (size_t)ns * SPN;
+  cplx *pool = calloc(fsz * (2 * n + 3), sizeof(cplx));
+  cplx **q1 = malloc(sizeof(cplx *) * n), **q2 = malloc(sizeof(cplx *) * n);
+  for (int i = 0; i < n; i++)
+  {
+    q1[i] = pool + fsz * i;
+    q2[i] = pool + fsz * (n + i);
+  }
+  cplx *p1 = pool + fsz * 2 * n, *p2 = p1 + fsz, *Mp = p2 + fsz, *tmp;
+  double *r = malloc(sizeof(double) * 5 * n), *s1 = r + n, *s2 = s1 + n, *c1 = s2 + n, *c2 = c1 + n;
+  short *flags = malloc(sizeof(short) * n);
+  int cgiter = 0, notconverged = n;
+  memcpy(p2, in, sizeof(cplx) * fsz);
+  const double innorm2 = orc_sqnorm(ns, in);
+  if (n == 1) /* out[0] is the start vector */
+  {
+    apply_op(op, Mp, out);
+    orc_mul_add_assign(ns, Mp, -shift[0], out);
+    la_sub(ns, p2, p2, Mp);
+  }
+  double rho = sqrt(orc_sqnorm(ns, p2));
+  la_mul(ns, p2, 1. / rho, p2);
+  memset(p1, 0, sizeof(cplx) * fsz);
+  for (int i = 0; i < n; i++)
+  {
+    r[i] = rho;
+    c2[i] = c1[i] = 1.;
+    s1[i] = s2[i] = 0.;
+    if (n != 1) memset(out + fsz * i, 0, sizeof(cplx) * fsz);
+    flags[i] = 1;
+  }
+  double delta = g5_prod_re_n(ns, p2, p2);
+  if (fabs(delta) < 1.e-28)
+  {
+    free(pool); free(q1); free(q2); free(r); free(flags);
+    return -1;
+  }
+  double beta = delta;
+  do
+  {
+    ++cgiter;
+    apply_op(op, Mp, p2);
+    orc_mul_add_assign(ns, Mp, -shift[0], p2);
+    const double alpha = g5_prod_re_n(ns, p2, Mp) / delta;
+    orc_mul_add_assign(ns, Mp, -beta, p1);
+    orc_mul_add_assign(ns, Mp, -alpha, p2);
+    tmp = p1; p1 = p2; p2 = Mp; Mp = tmp;
+    rho = sqrt(orc_sqnorm(ns, p2));
+    double maxm = 1.e-10;
+    for (int i = 0; i < n; i++)
+    {
+      if (!flags[i]) continue;
+      const double a = alpha - shift[i] + shift[0];
+      const double t = s1[i] * beta;
+      const double e = c2[i] * c1[i] * beta + s2[i] * a;
+      const double m = c2[i] * a - s2[i] * c1[i] * beta;
+      double d;
+      s1[i] = s2[i];
+      c1[i] = c2[i];
+      givens(&d, &c2[i], &s2[i], m, rho);
+      if (fabs(m) > maxm) maxm = fabs(m);
+      /* new direction q = d (p1 - t q1 - e q2), then the rotation q1 <- q2 <- q */
+      for (size_t k = 0; k < fsz; k++) Mp[k] = -t * d * q1[i][k] - e * d * q2[i][k];
+      orc_mul_add_assign(ns, Mp, d, p1);
+      tmp = q1[i]; q1[i] = q2[i]; q2[i] = Mp; Mp = tmp;
+      orc_mul_add_assign(ns, out + fsz * i, c2[i] * r[i], q2[i]);
+      r[i] *= -s2[i];
+      if (fabs(r[i] * r[i]) * (double)(1 + cgiter) < err2 * innorm2)
+      {
+        flags[i] = 0;
+        --notconverged;
+      }
+    }
+    if (fabs(rho) > 1.e-13)
+    {
+      la_mul(ns, p2, 1. / rho, p2);
+      const double olddelta = delta;
+      delta = g5_prod_re_n(ns, p2, p2);
+      if (fabs(delta) < 1.e-6 || maxm < 1.e-3) notconverged = 0; /* the method has failed */
+      beta = rho * delta / olddelta;
+    }
+    else
+      notconverged = 0; /* converged */
+  } while ((max_iter == 0 || cgiter < max_iter) && notconverged);
+  for (int i = 0; i < n; i++)
+  {
+    apply_op(op, Mp, out + fsz * i);
+    ++cgiter;
+    if (shift[i] != 0.) orc_mul_add_assign(ns, Mp, -shift[i], out + fsz * i);
+    la_sub(ns, Mp, Mp, in);
+    valid[i] = (fabs(orc_sqnorm(ns, Mp) / innorm2) > err2) ? 0 : 1;
+  }
+  if (n == 1) ++cgiter;
+  free(pool); free(q1); free(q2); free(r); free(flags);
+  return cgiter;
+}
+
+/* MINRES for a hermitian operator (LibHR/Inverters/MINRES.c:24-158).  The operator
+ * is g5 (M - sh) with M = op, the form g5QMR_mshift falls back to (g5QMR_mshift.c:466-474). */
+static int herm_op_, herm_g5_;
+static double herm_sh_;
+static void herm_apply(cplx *out, const cplx *in)
+{
+  const int ns = op_sites(herm_op_);
+  apply_op(herm_op_, out, in);
+  if (herm_sh_ != 0.) orc_mul_add_assign(ns, out, -herm_sh_, in);
+  if (herm_g5_) orc_g5(ns, out, out);
+}
+
+static int minres_core(short *valid, double err2, int max_iter, const cplx *in, cplx *out, const cplx *trial)
+{
+  const int ns = op_sites(herm_op_);
+  const size_t fsz = (size_t)ns * SPN;
+  cplx *pool = calloc(fsz * 5, sizeof(cplx));
+  cplx *q1 = pool, *q2 = q1 + fsz, *p1 = q2 + fsz, *p2 = p1 + fsz, *Mp = p2 + fsz, *tmp;
+  int cgiter = 0, notconverged = 1;
+  memcpy(p2, in, sizeof(cplx) * fsz);
+  if (trial)
+  {
+    herm_apply(p1, trial);
+    ++cgiter;
+    for (size_t k = 0; k < fsz; k++) p2[k] -= p1[k];
+    if (out != trial) memcpy(out, trial, sizeof(cplx) * fsz);
+  }
+  else
+    memset(out, 0, sizeof(cplx) * fsz);
+  const double innorm2 = orc_sqnorm(ns, in);
+  double beta = sqrt(orc_sqnorm(ns, p2));
+  la_mul(ns, p2, 1. / beta, p2);
+  memset(p1, 0, sizeof(cplx) * fsz);
+  double r = beta, rho2 = beta, rho1 = 1., c2 = -1., rp = 0., s1 = 0., s2 = 0., c1 = 0.;
+  do
+  {
+    ++cgiter;
+    herm_apply(Mp, p2);
+    const double alpha = orc_prod_re(ns, Mp, p2);
+    orc_mul_add_assign(ns, Mp, -beta, p1);
+    orc_mul_add_assign(ns, Mp, -alpha, p2);
+    tmp = p1; p1 = p2; p2 = Mp; Mp = tmp;
+    const double oldbeta = beta;
+    beta = sqrt(orc_sqnorm(ns, p2));
+    la_mul(ns, p2, 1. / beta, p2);
+    const double d = (alpha - rp * c1) * s2;
+    const double h = oldbeta * s1;
+    rp = -oldbeta * c1 * s2 - alpha * c2;
+    const double k = sqrt(rp * rp + beta * beta);
+    c1 = c2;
+    c2 = rp / k;
+    s1 = s2;
+    s2 = beta / k;
+    for (size_t q = 0; q < fsz; q++) Mp[q] = -h / rho1 * q1[q] - d / rho2 * q2[q];
+    tmp = q1; q1 = q2; q2 = tmp;
+    for (size_t q = 0; q < fsz; q++) q2[q] = p1[q] + Mp[q];
+    rho1 = rho2;
+    rho2 = k;
+    orc_mul_add_assign(ns, out, r * c2 / k, q2);
+    r *= s2;
+    if (r * r < err2 * innorm2) notconverged = 0;
+  } while ((max_iter == 0 || cgiter < max_iter) && notconverged);
+  herm_apply(Mp, out);
+  ++cgiter;
+  la_sub(ns, Mp, Mp, in);
+  *valid = (fabs(orc_sqnorm(ns, Mp) / innorm2) > err2) ? 0 : 1;
+  free(pool);
+  return cgiter;
+}
+
+/* MINRES (MINRES.c:160-172): repeated from the last solution until valid (bounded here) */
+int orc_MINRES(int op, int g5, double sh, double err2, int max_iter, const cplx *in, cplx *out, const cplx *trial)
+{
+  herm_op_ = op;
+  herm_g5_ = g5;
+  herm_sh_ = sh;
+  short valid;
+  int iter = minres_core(&valid, err2, max_iter, in, out, trial), rep = 0;
+  while (!valid && (max_iter == 0 || iter < max_iter) && ++rep < 100) iter += minres_core(&valid, err2, max_iter, in, out, out);
+  return iter;
+}
+
+/* g5QMR_mshift (g5QMR_mshift.c:481-542): unconverged shifts are solved again one at a
+ * time from their current solution, then with MINRES on g5 (M - shift). */
+int orc_g5QMR_mshift(int op, int n, const double *shift, double err2, int max_iter, const cplx *in, cplx *out)
+{
+  const int ns = op_sites(op);
+  const size_t fsz = (size_t)ns * SPN;
+  short valid[n > 0 ? n : 1];
+  int cgiter = g5qmr_core(valid, op, n, shift, err2, max_iter, in, out);
+  if (cgiter < 0) return -1;
+  for (int i = 0; i < n; i++)
+  {
+    if (valid[i]) continue;
+    int it = g5qmr_core(valid + i, op, 1, shift + i, err2, 0, in, out + fsz * i);
+    if (it < 0) return -1;
+    cgiter += it;
+    if (!valid[i])
+    {
+      cplx *g5in = malloc(sizeof(cplx) * fsz);
+      orc_g5(ns, g5in, in);
+      cgiter += orc_MINRES(op, 1, shift[i], err2, 0, g5in, out + fsz * i, out + fsz * (i == 0 ? 0 : i - 1));
+      free(g5in);
+    }
+  }
+  return cgiter;
+}
+
+/* ------------------------------------------------------------------------- */
+/* chronological initial guess (MRE): LibHR/Update/mre.c                      */
+/* ------------------------------------------------------------------------- */
+/* in-place LU with partial pivoting of A (max x max, row-major) and solution of
+ * A x = conj(b) (mre.c:56-143) */
+static int mre_lu_solve(int max, cplx *A, const cplx *b, cplx *x)
+{
+  int mutate[64];
+  cplx y[64];
+  for (int i = 0; i < max; i++) mutate[i] = i;
+  for (int i = 0; i < max; i++)
+  {
+    for (int j = 0; j <= i; j++)
+      for (int k = 0; k < j; k++) A[j * max + i] -= A[j * max + k] * A[k * max + i];
+    double big = cabs(A[i * max + i]);
+    int row = i;
+    for (int j = i + 1; j < max; j++)
+    {
+      for (int k = 0; k < i; k++) A[j * max + i] -= A[j * max + k] * A[k * max + i];
+      if (cabs(A[j * max + i]) > big)
+      {
+        big = cabs(A[j * max + i]);
+        row = j;
+      }
+    }
+    if (big < 1.0e-14) return -1; /* singular: HiRep keeps the previous x */
+    if (row != i)
+    {
+      for (int k = 0; k < max; k++)
+      {
+        cplx t = A[row * max + k];
+        A[row * max + k] = A[i * max + k];
+        A[i * max + k] = t;
+      }
+      int t = mutate[row];
+      mutate[row] = mutate[i];
+      mutate[i] = t;
+    }
+    for (int k = i + 1; k < max; k++) A[k * max + i] = A[k * max + i] / A[i * max + i];
+  }
+  for (int i = 0; i < max; i++)
+  {
+    y[i] = conj(b[mutate[i]]);
+    for (int k = 0; k < i; k++) y[i] -= A[i * max + k] * y[k];
+  }
+  for (int i = max - 1; i >= 0; i--)
+  {
+    x[i] = y[i];
+    for (int k = i + 1; k < max; k++) x[i] -= A[i * max + k] * x[k];
+    x[i] = x[i] / A[i * max + i];
+  }
+  return 0;
+}
+
+/* mre_guess (mre.c:230-268): s holds the `max` most recent solutions (newest
+ * first); out = sum_i x_i v_i over their Gram-Schmidt basis v_i, with
+ * A[j][i] = <DD v_i, v_j>, b_i = <v_i, pf> */
+void orc_mre_guess(int op, int max, const cplx *s, cplx *out, const cplx *pf)
+{
+  const int ns = op_sites(op);
+  const size_t fsz = (size_t)ns * SPN;
+  memset(out, 0, sizeof(cplx) * fsz);
+  if (max <= 0) return;
+  cplx *v = malloc(sizeof(cplx) * fsz * (max + 1)), *Dv = v + fsz * max;
+  memcpy(v, s, sizeof(cplx) * fsz * max);
+  for (int i = 0; i < max; i++) /* gram_schmidt (mre.c:30-48) */
+  {
+    cplx *vi = v + fsz * i;
+    la_mul(ns, vi, 1.0 / sqrt(orc_sqnorm(ns, vi)), vi);
+    for (int j = i + 1; j < max; j++)
+    {
+      cplx *vj = v + fsz * j;
+      cplx rij = orc_prod_re(ns, vi, vj) + I * orc_prod_im(ns, vi, vj);
+      for (size_t q = 0; q < fsz; q++) vj[q] -= rij * vi[q];
+    }
+  }
+  cplx A[64 * 64], b[64], x[64];
+  for (int i = 0; i < max; i++)
+  {
+    apply_op(op, Dv, v + fsz * i);
+    for (int j = 0; j < max; j++) A[j * max + i] = orc_prod_re(ns, Dv, v + fsz * j) + I * orc_prod_im(ns, Dv, v + fsz * j);
+    b[i] = orc_prod_re(ns, v + fsz * i, pf) + I * orc_prod_im(ns, v + fsz * i, pf);
+  }
+  if (mre_lu_solve(max, A, b, x) == 0)
+    for (int i = 0; i < max; i++)
+      for (size_t q = 0; q < fsz; q++) out[q] += x[i] * v[fsz * i + q];
+  free(v);
 }
 
 /* ------------------------------------------------------------------------- */

@@ -100,11 +100,21 @@ void orc_gamma(int mu, int n, double complex *s1, const double complex *s2);
 float orc_sqnorm_flt_site(const float complex *s);
 
 /* inverters (LibHR/Inverters/cg_mshift.c, cg_mshift_flt.c) */
-enum { ORC_OP_G5DPHI_SQ = 0, ORC_OP_G5DPHI_EOPRE_SQ = 1, ORC_OP_G5CPHI_EOPRE_SQ = 2, ORC_OP_G5CPHI_SQ = 3 };
+enum {
+  ORC_OP_G5DPHI_SQ = 0, ORC_OP_G5DPHI_EOPRE_SQ = 1, ORC_OP_G5CPHI_EOPRE_SQ = 2, ORC_OP_G5CPHI_SQ = 3,
+  ORC_OP_DPHI_EOPRE = 4, ORC_OP_G5DPHI_EOPRE = 5, ORC_OP_CPHI_EOPRE = 6, ORC_OP_G5CPHI_EOPRE = 7,
+  ORC_OP_DPHI = 8, ORC_OP_CPHI = 9
+};
 int orc_cg_mshift(int op, int n, const double *shift, double err2, int max_iter,
                   const double complex *in, double complex *out);
 int orc_cg_mshift_flt(int op, int n, const double *shift, double err2, int max_iter,
                       const double complex *in, double complex *out);
+/* g5QMR_mshift, MINRES (LibHR/Inverters/g5QMR_mshift.c, MINRES.c) and the MRE guess (LibHR/Update/mre.c) */
+int orc_g5QMR_mshift(int op, int n, const double *shift, double err2, int max_iter,
+                     const double complex *in, double complex *out);
+int orc_MINRES(int op, int g5, double sh, double err2, int max_iter, const double complex *in,
+               double complex *out, const double complex *trial);
+void orc_mre_guess(int op, int max, const double complex *s, double complex *out, const double complex *pf);
 
 /* force (LibHR/Update/force_fermion_core.c) */
 void orc_fermion_force_begin(void);

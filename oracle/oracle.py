@@ -21,6 +21,7 @@ _LIB_PATH = os.path.join(_HERE, "_build", "libhroracle.so")
 FUND, ADJ, SYM, ASYM = 0, 1, 2, 3
 EVEN, ODD, FULL = 0, 1, 2
 OP_G5DPHI_SQ, OP_G5DPHI_EOPRE_SQ, OP_G5CPHI_EOPRE_SQ, OP_G5CPHI_SQ = 0, 1, 2, 3
+OP_DPHI_EOPRE, OP_G5DPHI_EOPRE, OP_CPHI_EOPRE, OP_G5CPHI_EOPRE, OP_DPHI, OP_CPHI = 4, 5, 6, 7, 8, 9
 REPR_NAMES = {"FUND": FUND, "ADJ": ADJ, "SYM": SYM, "ASYM": ASYM}
 
 
@@ -256,6 +257,37 @@ class Oracle:
         if it < 0:
             raise ValueError("oracle: operator has no float version")
         return out, it
+
+    def g5QMR_mshift(self, op, shifts, err2, inp, max_iter=0, guess=None):
+        """g5QMR_mshift (LibHR/Inverters/g5QMR_mshift.c:481-542); op is the gamma_5-hermitian M."""
+        inp = self._c(inp)
+        n = len(shifts)
+        sh = np.ascontiguousarray(shifts, np.float64)
+        out = np.zeros((n,) + inp.shape, np.complex128)
+        if guess is not None:
+            out[0] = guess
+        it = self.L.orc_g5QMR_mshift(op, n, _p(sh), ctypes.c_double(err2), max_iter, _p(inp), _p(out))
+        if it < 0:
+            raise ValueError("oracle g5QMR: gamma_5 norm of the start vector is zero")
+        return out, it
+
+    def MINRES(self, op, err2, inp, trial=None, max_iter=0, g5=False, sh=0.0):
+        """MINRES (LibHR/Inverters/MINRES.c:160-172) on the hermitian operator
+        op - sh, or g5 (op - sh) when g5 is set."""
+        inp = self._c(inp)
+        out = np.zeros_like(inp)
+        tr = None if trial is None else self._c(trial)
+        it = self.L.orc_MINRES(op, int(bool(g5)), ctypes.c_double(sh), ctypes.c_double(err2), max_iter, _p(inp),
+                               _p(out), None if tr is None else _p(tr))
+        return out, it
+
+    def mre_guess(self, op, solutions, pf):
+        """mre_guess (LibHR/Update/mre.c:230-268) from past solutions (newest first)."""
+        pf = self._c(pf)
+        s = np.ascontiguousarray(np.asarray(solutions, np.complex128))
+        out = np.zeros_like(pf)
+        self.L.orc_mre_guess(op, len(solutions), _p(s), _p(out), _p(pf))
+        return out
 
     # force ---------------------------------------------------------------
     def fermion_force_begin(self):

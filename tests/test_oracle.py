@@ -244,3 +244,71 @@ def test_smooth_field_plaquette():
     u = F.smooth_gauge(7, o.V, 3, 0.3)
     p = o.avr_plaquette(u)
     assert 0.7 < p < 0.9
+
+
+# ---- g5QMR_mshift, MINRES, MRE (LibHR/Inverters/g5QMR_mshift.c, MINRES.c, LibHR/Update/mre.c)
+SHIFTS6 = [0.1, -0.21, 0.05, -0.01, -0.15, -0.05]  # check_inverters_2.c:83-88, check_inverters_3.c:73-78
+
+
+@pytest.mark.parametrize("op", [O.OP_DPHI_EOPRE, O.OP_DPHI])
+def test_g5qmr_six_shifts(op):
+    """check_inverters_3.c: g5QMR_mshift on D with six shifts, |D x - s x - b|^2/|b|^2 < err2."""
+    o = O.Oracle(4, 4, 4, 4, 3, O.FUND)
+    o.set_gauge(o.represent_gauge_field(F.hot_gauge(1234, o.V, 3), True))
+    o.set_mass(0.1)
+    par = O.FULL if op == O.OP_DPHI else O.EVEN
+    b = F.gaussian_spinor(5, o.nsites(par), o.nf)
+    err2 = 1e-26
+    x, it = o.g5QMR_mshift(op, SHIFTS6, err2, b)
+    D = o.Dphi if op == O.OP_DPHI else o.Dphi_eopre
+    for i, s in enumerate(SHIFTS6):
+        r = D(0.1, x[i]) - s * x[i] - b
+        assert o.sqnorm(r) / o.sqnorm(b) < err2, (i, s)
+    assert it > 0
+
+
+def test_minres_hermitian_g5D():
+    """check_inverters_2.c:111-141: MINRES on H = g5 D(m) with the mass moved by -shift,
+    i.e. g5 (D - shift), each solve started from the previous solution."""
+    o = O.Oracle(4, 4, 4, 4, 3, O.FUND)
+    o.set_gauge(o.represent_gauge_field(F.hot_gauge(1234, o.V, 3), True))
+    o.set_mass(0.1)
+    b = F.gaussian_spinor(6, o.VH, o.nf)
+    err2 = 1e-26
+    prev = None
+    for s in [0.0] + SHIFTS6[:-1]:
+        x, it = o.MINRES(O.OP_DPHI_EOPRE, err2, b, trial=prev, g5=True, sh=s)
+        r = o.gamma(5, o.Dphi_eopre(0.1, x) - s * x) - b
+        assert o.sqnorm(r) / o.sqnorm(b) < err2
+        prev = x
+
+
+def _mre_numpy(o, D, sols, pf):
+    """HiRep's mre_guess formula restated with numpy (Gram-Schmidt, A[j][i] = <D v_i, v_j>,
+    b_i = <v_i, pf>, A y = conj(b), out = sum y_i v_i)."""
+    v = [s.copy() for s in sols]
+    for i in range(len(v)):
+        v[i] = v[i] / np.sqrt(np.vdot(v[i], v[i]).real)
+        for j in range(i + 1, len(v)):
+            v[j] = v[j] - np.vdot(v[i], v[j]) * v[i]
+    n = len(v)
+    A = np.empty((n, n), complex)
+    bb = np.empty(n, complex)
+    for i in range(n):
+        Dv = D(v[i])
+        for j in range(n):
+            A[j, i] = np.vdot(Dv, v[j])
+        bb[i] = np.vdot(v[i], pf)
+    y = np.linalg.solve(A, np.conj(bb))
+    return sum(y[i] * v[i] for i in range(n))
+
+
+def test_mre_guess_formula():
+    o = O.Oracle(4, 4, 4, 4, 3, O.FUND)
+    o.set_gauge(o.represent_gauge_field(F.smooth_gauge(3, o.V, 3, 0.3), True))
+    o.set_mass(0.1)
+    sols = [F.gaussian_spinor(20 + k, o.VH, o.nf) for k in range(5)]
+    pf = F.gaussian_spinor(30, o.VH, o.nf)
+    g = o.mre_guess(O.OP_DPHI_EOPRE, sols, pf)
+    ref = _mre_numpy(o, lambda s: o.Dphi_eopre(0.1, s), sols, pf)
+    assert np.abs(g - ref).max() / np.abs(ref).max() < 1e-12
