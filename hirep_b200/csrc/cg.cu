@@ -229,6 +229,7 @@ static int cg_workspace(int prec, int nvec, size_t bytes) {
 void cg_release() {
   batch_release();
   qmr_release();
+  hmc_release();
   cudaFree(FW.dres); cudaFree(FW.dres2); cudaFree(FW.dtmp);
   for (void *b : FW.fbuf) cudaFree(b);
   FW = FltWork();

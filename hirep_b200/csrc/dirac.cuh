@@ -23,6 +23,8 @@ double static_mass();
 void add_mvm(unsigned long n);  // hops done outside hop(), e.g. replayed CUDA graphs
 void batch_release();           // batch.cu: workspaces and captured graphs
 void qmr_release();             // qmr.cu: the g5QMR / MINRES work fields
+void hmc_release();             // hmc.cu: generators, local action
+int fermion_force_finish(double dt);  // force.cu: clover part of fermion_force_end
 
 // clover: make sure the packed (4+m)+A blocks and their inverse exist for this
 // mass in this precision (the LDL cache of clover_tools.c:343-358)

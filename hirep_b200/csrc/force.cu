@@ -304,6 +304,22 @@ int links_out(void *host, const void *dev, int nel, int elem_bytes, int ndir);
 
 }  // namespace hrgpu
 
+namespace hrgpu {
+
+// the clover part of fermion_force_end (force_fermion_core.c:964-984), into force_sum
+int fermion_force_finish(double dt) {
+  if (!L.clover) return 0;
+  if (int rc = check_gauge(HRGPU_DOUBLE)) return rc;
+  const double coeff = dt * (L.repr_norm2 / L.fund_norm2) * (1. / 8.) * L.csw;
+  Geo g = make_geo();
+  const long n = 2L * L.ld;
+  HR_NF_DISPATCH(L.real, L.nf, (k_force_clover_core<N_, R_><<<dim3(nb(n, 64), 4), 64, 0, L.stream>>>(L.force_sum, L.U, L.cl_force, g, proj(), coeff)));
+  HR_LAUNCH_CHECK();
+  return 0;
+}
+
+}  // namespace hrgpu
+
 using namespace hrgpu;
 
 extern "C" {
@@ -362,14 +378,7 @@ int hrgpu_force_clover_logdet(double mass, double residue) {
 int hrgpu_fermion_force_end(double dt, double *force_host) {
   HR_REQUIRE(L.ready && L.force_sum, HRGPU_E_STATE, "fermion_force_end: no force accumulated");
   HR_REQUIRE(force_host, HRGPU_E_ARG, "fermion_force_end: NULL force field");
-  if (L.clover) {
-    if (int rc = check_gauge(HRGPU_DOUBLE)) return rc;
-    const double coeff = dt * (L.repr_norm2 / L.fund_norm2) * (1. / 8.) * L.csw;
-    Geo g = make_geo();
-    const long n = 2L * L.ld;
-    HR_NF_DISPATCH(L.real, L.nf, (k_force_clover_core<N_, R_><<<dim3(nb(n, 64), 4), 64, 0, L.stream>>>(L.force_sum, L.U, L.cl_force, g, proj(), coeff)));
-    HR_LAUNCH_CHECK();
-  }
+  if (int rc = fermion_force_finish(dt)) return rc;
   const size_t m = (size_t)L.V * 4 * L.dimg;
   double *tmp = new double[m];
   int rc = links_out(tmp, L.force_sum, L.dimg, 8, 4);

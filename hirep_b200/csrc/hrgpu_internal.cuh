@@ -79,8 +79,10 @@ struct Lattice {
   float2 *cl_od_f = nullptr, *cl_iod_f = nullptr;
   double sigma_diag = 0xF00F;     // mass term the packed diag was built for
   double sigma_flt = 0xF00F;
-  // force
+  // force and HMC
   double *force_sum = nullptr;    // [4][dimg][2*ld]
+  double *mom = nullptr;          // momenta [4][dimg][2*ld]
+  int bc_t = 1;                   // time boundary condition of the last represent_gauge_field
   double2 *cl_force = nullptr;    // [6][nf*nf][2*ld]
   // algebra projection tables (sparse): for each generator A, entries (k=i*nf+j, coeff)
   int *d_proj_off = nullptr;      // [dimg+1]

@@ -138,6 +138,7 @@ int hrgpu_represent_gauge_field(int bc_t_antiperiodic) {
   k_represent<<<dim3((unsigned)((n + 127) / 128), 4), 128, 0, L.stream>>>(L.U, L.Ug, L.ng, L.repr, g, bc_t_antiperiodic);
   HR_LAUNCH_CHECK();
   L.have_gauge = true;
+  L.bc_t = bc_t_antiperiodic;
   if (int rc = hrgpu_assign_ud2u_f()) return rc;
   if (L.clover) {
     if (int rc = compute_clover_term_dev()) return rc;

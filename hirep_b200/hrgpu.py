@@ -324,6 +324,55 @@ class Lattice:
             raise HRGPUError("mre_init: " + self.L.hrgpu_last_error().decode())
         return MREHandle(self, ctypes.c_void_p(h))
 
+    # HMC pieces -----------------------------------------------------------------
+    def momenta_set(self, mom):
+        mom = np.ascontiguousarray(mom, np.float64)
+        assert mom.shape == (self.V, 4, self.dimg)
+        _check(self.L.hrgpu_momenta_set(_ptr(mom)), "momenta_set")
+
+    def momenta_get(self):
+        mom = np.empty((self.V, 4, self.dimg), np.float64)
+        _check(self.L.hrgpu_momenta_get(_ptr(mom)), "momenta_get")
+        return mom
+
+    def gauge_get(self):
+        u = np.empty((self.V, 4, self.ng, self.ng), np.complex128)
+        _check(self.L.hrgpu_gauge_get(_ptr(u)), "gauge_get")
+        return u
+
+    def force0(self, dt, beta):
+        _check(self.L.hrgpu_force0(D(dt), D(beta)), "force0")
+
+    def update_gauge_field(self, dt):
+        _check(self.L.hrgpu_update_gauge_field(D(dt)), "update_gauge_field")
+
+    def project_gauge_field(self):
+        _check(self.L.hrgpu_project_gauge_field(), "project_gauge_field")
+
+    def local_hmc_action(self, delta, beta):
+        _check(self.L.hrgpu_local_hmc_action(int(bool(delta)), D(beta)), "local_hmc_action")
+
+    def pf_local_action(self, pf):
+        _check(self.L.hrgpu_pf_local_action(pf.ptr, pf.par), "pf_local_action")
+
+    def local_action_sum(self):
+        s = ctypes.c_double()
+        _check(self.L.hrgpu_local_action_sum(ctypes.byref(s)), "local_action_sum")
+        return s.value
+
+    def local_action(self):
+        loc = np.empty(self.V, np.float64)
+        _check(self.L.hrgpu_local_action_get(_ptr(loc)), "local_action_get")
+        return loc
+
+    def avr_plaquette(self):
+        p = ctypes.c_double()
+        _check(self.L.hrgpu_avr_plaquette(ctypes.byref(p)), "avr_plaquette")
+        return p.value
+
+    def fermion_force_end_momenta(self, dt):
+        _check(self.L.hrgpu_fermion_force_end_momenta(D(dt)), "fermion_force_end_momenta")
+
     # many right-hand sides -------------------------------------------------------
     def batch(self, nb, prec=DOUBLE, fields=None):
         b = Batch(self, nb, prec)

@@ -257,6 +257,38 @@ int hrgpu_mre_store(void *mre, int p, const void *in);
 int hrgpu_mre_guess(void *mre, int p, void *out, int op, double mass, const void *pf);
 int hrgpu_mre_free(void *mre);
 
+/* ------------------------------------------------------------ HMC pieces -- */
+/* The gauge-side pieces of an HMC step on the device (HiRep's drivers --
+ * integrator, monomials, accept/reject -- stay host code calling these).
+ * Momenta: HiRep's suN_momenta, host layout [V][4][NG*NG-1] in HiRep's site
+ * order; the library keeps one device copy. */
+int hrgpu_momenta_set(const double *host);
+int hrgpu_momenta_get(double *host);
+/* the fundamental links, host layout of hrgpu_gauge_set */
+int hrgpu_gauge_get(double *u_host);
+/* force0 (LibHR/Update/force0.c:22-99): momenta += -dt beta/NG proj(U staples^+) */
+int hrgpu_force0(double dt, double beta);
+/* update_gauge_field (LibHR/Update/field_update.c:18-66): U <- exp(dt mom) U on
+ * every link (ExpX), reunitarised every 17th call (project_to_suNg,
+ * suN_utils.c:76-150), then represent_gauge_field (and the clover term) with the
+ * time boundary condition of the last hrgpu_represent_gauge_field */
+int hrgpu_update_gauge_field(double dt);
+int hrgpu_project_gauge_field(void);
+/* local_hmc_action (LibHR/Update/local_action.c:19-90) into a device per-site
+ * field: NEW sets it to 1/2 C(F) |mom|^2 - beta/NG (sum of the 6 plaquettes),
+ * DELTA to that minus its previous content; pf_local_action adds |pf|^2 of a
+ * pseudofermion of parity par; local_action_sum returns the sum over sites
+ * (fixed-order reduction) and local_action_get the field ([V], HiRep order). */
+enum { HRGPU_ACTION_NEW = 0, HRGPU_ACTION_DELTA = 1 };
+int hrgpu_local_hmc_action(int type, double beta);
+int hrgpu_pf_local_action(const void *pf, int par);
+int hrgpu_local_action_sum(double *sum);
+int hrgpu_local_action_get(double *host);
+/* avr_plaquette (LibHR/Observables/avr_plaquette.c): mean of Re Tr P / NG */
+int hrgpu_avr_plaquette(double *plaq);
+/* fermion_force_end (force_fermion_core.c:964-993) adding into the device momenta */
+int hrgpu_fermion_force_end_momenta(double dt);
+
 /* ------------------------------------------------------ batched (multi-RHS) -- */
 /* HiRep has no batched interface; these entry points serve its callers that
  * hold many sources at once (calc_prop.c:210-289 loops cg_mshift over the 4*NF

@@ -2140,6 +2140,218 @@ void orc_get_clover_force(cplx *cf) { memcpy(cf, cl_force_, sizeof(cplx) * V_ * 
 /* average plaquette (LibHR/Observables/avr_plaquette.c:29-53,92)            */
 /* fundamental links u[4*ix+mu] NG x NG                                       */
 /* ------------------------------------------------------------------------- */
+/* ------------------------------------------------------------------------- */
+/* HMC pieces: gauge force (LibHR/Update/force0.c:22-99, staples.c:22-70),    */
+/* link update (field_update.c:18-66, ExpX in suN_exp_group.c:358-378),       */
+/* reunitarisation (suN_utils.c:76-150), local action (local_action.c:19-90,  */
+/* mon_pg.c:36-43).  Fundamental links u[V][4][NG*NG], momenta [V][4][DIMG].  */
+/* ------------------------------------------------------------------------- */
+static void mat_mul_dag(int n, cplx *c, const cplx *a, const cplx *b) /* c = a b^+ */
+{
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++)
+    {
+      cplx t = 0;
+      for (int k = 0; k < n; k++) t += a[i * n + k] * conj(b[j * n + k]);
+      c[i * n + j] = t;
+    }
+}
+static void mat_dag_mul(int n, cplx *c, const cplx *a, const cplx *b) /* c = a^+ b */
+{
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++)
+    {
+      cplx t = 0;
+      for (int k = 0; k < n; k++) t += conj(a[k * n + i]) * b[k * n + j];
+      c[i * n + j] = t;
+    }
+}
+
+/* sum of the six staples around link (ix, mu) (staples.c:22-70) */
+static void staple_sum(cplx *v, const cplx *u, int ix, int mu)
+{
+  const int N = NG_, N2 = NG_ * NG_;
+  cplx t1[N2], t2[N2];
+  for (int k = 0; k < N2; k++) v[k] = 0;
+  const int ixpmu = iup_[4 * ix + mu];
+  for (int i = 1; i < 4; i++)
+  {
+    const int nu = (mu + i) & 3;
+    const int ixpnu = iup_[4 * ix + nu], ixmnu = idn_[4 * ix + nu], ixpmumnu = idn_[4 * ixpmu + nu];
+#define UL(x, m) (u + ((size_t)(x) * 4 + (m)) * N2)
+    /* up: U(x,nu) U(x+nu,mu) U(x+mu,nu)^+ */
+    mat_mul(N, t2, UL(ix, nu), UL(ixpnu, mu));
+    mat_mul_dag(N, t1, t2, UL(ixpmu, nu));
+    for (int k = 0; k < N2; k++) v[k] += t1[k];
+    /* down: U(x-nu,nu)^+ U(x-nu,mu) U(x+mu-nu,nu) */
+    mat_mul(N, t2, UL(ixmnu, mu), UL(ixpmumnu, nu));
+    mat_dag_mul(N, t1, UL(ixmnu, nu), t2);
+    for (int k = 0; k < N2; k++) v[k] += t1[k];
+#undef UL
+  }
+}
+
+/* force0: mom(x,mu) += (-dt beta / NG) proj(U(x,mu) S(x,mu)^+) */
+void orc_force0(double dt, double beta, const cplx *u, double *mom)
+{
+  const int N = NG_, N2 = NG_ * NG_;
+  const double coeff = -dt * beta / N;
+#pragma omp parallel for
+  for (int ix = 0; ix < V_; ix++)
+  {
+    cplx st[N2], w[N2];
+    double f[DIMG_];
+    for (int mu = 0; mu < 4; mu++)
+    {
+      staple_sum(st, u, ix, mu);
+      mat_mul_dag(N, w, u + ((size_t)ix * 4 + mu) * N2, st);
+      orc_fund_algebra_project(f, w);
+      for (int A = 0; A < DIMG_; A++) mom[((size_t)ix * 4 + mu) * DIMG_ + A] += coeff * f[A];
+    }
+  }
+}
+
+/* e = exp(x) for an NG x NG matrix with small norm: scaling and squaring of
+ * the Taylor series (the reference's suNg_Exp is exact to rounding as well) */
+static void mat_exp(int n, cplx *e, const cplx *x)
+{
+  const int n2 = n * n;
+  double nrm = 0;
+  for (int k = 0; k < n2; k++) nrm += creal(x[k] * conj(x[k]));
+  nrm = sqrt(nrm);
+  int sq = 0;
+  while (nrm > 0.25)
+  {
+    nrm *= 0.5;
+    sq++;
+  }
+  const double scale = ldexp(1.0, -sq);
+  cplx a[n2], term[n2], tmp[n2];
+  for (int k = 0; k < n2; k++)
+  {
+    a[k] = x[k] * scale;
+    e[k] = (k % (n + 1) == 0) ? 1.0 : 0.0;
+    term[k] = e[k];
+  }
+  for (int j = 1; j <= 20; j++)
+  {
+    mat_mul(n, tmp, term, a);
+    for (int k = 0; k < n2; k++)
+    {
+      term[k] = tmp[k] / j;
+      e[k] += term[k];
+    }
+  }
+  for (int q = 0; q < sq; q++)
+  {
+    mat_mul(n, tmp, e, e);
+    memcpy(e, tmp, sizeof(cplx) * n2);
+  }
+}
+
+/* U(x,mu) <- exp(dt X(mom(x,mu))) U(x,mu), X = sum_A mom_A iT_A (ExpX) */
+void orc_update_gauge_field(double dt, cplx *u, const double *mom)
+{
+  const int N = NG_, N2 = NG_ * NG_;
+#pragma omp parallel for
+  for (int l = 0; l < 4 * V_; l++)
+  {
+    cplx x[N2], e[N2], t[N2];
+    orc_fund_algebra_represent(x, mom + (size_t)l * DIMG_);
+    for (int k = 0; k < N2; k++) x[k] *= dt;
+    mat_exp(N, e, x);
+    mat_mul(N, t, e, u + (size_t)l * N2);
+    memcpy(u + (size_t)l * N2, t, sizeof(cplx) * N2);
+  }
+}
+
+/* project_to_suNg (suN_utils.c:76-150): Gram-Schmidt of the rows, then the
+ * determinant's phase removed with det^(-1/NG) (principal branch) */
+static cplx mat_det(int n, const cplx *m)
+{
+  cplx a[n * n], d = 1;
+  memcpy(a, m, sizeof(cplx) * n * n);
+  for (int i = 0; i < n; i++)
+  {
+    int p = i;
+    for (int r = i + 1; r < n; r++)
+      if (cabs(a[r * n + i]) > cabs(a[p * n + i])) p = r;
+    if (p != i)
+    {
+      for (int k = 0; k < n; k++)
+      {
+        cplx t = a[i * n + k];
+        a[i * n + k] = a[p * n + k];
+        a[p * n + k] = t;
+      }
+      d = -d;
+    }
+    if (a[i * n + i] == 0) return 0;
+    d *= a[i * n + i];
+    for (int r = i + 1; r < n; r++)
+    {
+      cplx f = a[r * n + i] / a[i * n + i];
+      for (int k = i; k < n; k++) a[r * n + k] -= f * a[i * n + k];
+    }
+  }
+  return d;
+}
+
+void orc_project_gauge_field(cplx *u)
+{
+  const int N = NG_, N2 = NG_ * NG_;
+#pragma omp parallel for
+  for (int l = 0; l < 4 * V_; l++)
+  {
+    cplx *m = u + (size_t)l * N2;
+    double nrm = 0;
+    for (int k = 0; k < N2; k++) nrm += creal(m[k] * conj(m[k]));
+    if (nrm < 1.e-28) continue;
+    for (int i = 0; i < N; i++)
+    {
+      cplx *vi = m + i * N;
+      for (int j = 0; j < i; j++)
+      {
+        const cplx *vj = m + j * N;
+        cplx z = 0;
+        for (int k = 0; k < N; k++) z += conj(vj[k]) * vi[k];
+        for (int k = 0; k < N; k++) vi[k] -= z * vj[k];
+      }
+      double q = 0;
+      for (int k = 0; k < N; k++) q += creal(vi[k] * conj(vi[k]));
+      q = 1.0 / sqrt(q);
+      for (int k = 0; k < N; k++) vi[k] *= q;
+    }
+    cplx f = cpow(mat_det(N, m), -1.0 / N);
+    for (int k = 0; k < N2; k++) m[k] *= f;
+  }
+}
+
+/* local action per site (local_action.c:19-90, mon_pg.c:36-43):
+ * 0.5 * C(F) * sum_mu |mom(x,mu)|^2 - beta/NG * (sum of the 6 plaquettes at x) */
+void orc_local_hmc_action(double beta, const cplx *u, const double *mom, double *loc)
+{
+  const int N = NG_, N2 = NG_ * NG_;
+#pragma omp parallel for
+  for (int ix = 0; ix < V_; ix++)
+  {
+    double a = 0;
+    for (int q = 0; q < 4 * DIMG_; q++) a += mom[(size_t)ix * 4 * DIMG_ + q] * mom[(size_t)ix * 4 * DIMG_ + q];
+    a *= 0.5 * fund_norm2_;
+    cplx w1[N2], w2[N2];
+    double pl = 0;
+    for (int mu = 1; mu < 4; mu++)
+      for (int nu = 0; nu < mu; nu++)
+      {
+        mat_mul(N, w1, u + ((size_t)ix * 4 + mu) * N2, u + ((size_t)iup_[4 * ix + mu] * 4 + nu) * N2);
+        mat_mul(N, w2, u + ((size_t)ix * 4 + nu) * N2, u + ((size_t)iup_[4 * ix + nu] * 4 + mu) * N2);
+        for (int i = 0; i < N; i++)
+          for (int k = 0; k < N; k++) pl += creal(w1[i * N + k] * conj(w2[i * N + k]));
+      }
+    loc[ix] = a - beta / N * pl;
+  }
+}
+
 double orc_avr_plaquette(const cplx *u)
 {
   int N = NG_;

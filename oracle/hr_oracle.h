@@ -124,6 +124,12 @@ void orc_fermion_force_end(double dt, double *force);
 void orc_get_force_sum(double *f);
 void orc_get_clover_force(double complex *cf);
 
+/* HMC pieces (LibHR/Update/force0.c, staples.c, field_update.c, local_action.c, suN_utils.c) */
+void orc_force0(double dt, double beta, const double complex *u, double *mom);
+void orc_update_gauge_field(double dt, double complex *u, const double *mom);
+void orc_project_gauge_field(double complex *u);
+void orc_local_hmc_action(double beta, const double complex *u, const double *mom, double *loc);
+
 /* gauge utilities used by tests */
 double orc_avr_plaquette(const double complex *u);
 

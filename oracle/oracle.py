@@ -289,6 +289,34 @@ class Oracle:
         self.L.orc_mre_guess(op, len(solutions), _p(s), _p(out), _p(pf))
         return out
 
+    # HMC pieces ------------------------------------------------------------
+    def force0(self, dt, beta, u, mom):
+        """force0 (LibHR/Update/force0.c:22-99): mom += -dt beta/NG proj(U staples^+); returns mom."""
+        u = np.ascontiguousarray(u, np.complex128)
+        mom = np.ascontiguousarray(mom, np.float64).copy()
+        self.L.orc_force0(ctypes.c_double(dt), ctypes.c_double(beta), _p(u), _p(mom))
+        return mom
+
+    def update_gauge_field(self, dt, u, mom):
+        """U <- exp(dt X(mom)) U on every link (field_update.c:18-66, ExpX); returns U."""
+        u = np.ascontiguousarray(u, np.complex128).copy()
+        mom = np.ascontiguousarray(mom, np.float64)
+        self.L.orc_update_gauge_field(ctypes.c_double(dt), _p(u), _p(mom))
+        return u
+
+    def project_gauge_field(self, u):
+        u = np.ascontiguousarray(u, np.complex128).copy()
+        self.L.orc_project_gauge_field(_p(u))
+        return u
+
+    def local_hmc_action(self, beta, u, mom):
+        """per-site 0.5 C(F) |mom|^2 - beta/NG (6 plaquettes) (local_action.c, mon_pg.c)"""
+        u = np.ascontiguousarray(u, np.complex128)
+        mom = np.ascontiguousarray(mom, np.float64)
+        loc = np.zeros(self.V, np.float64)
+        self.L.orc_local_hmc_action(ctypes.c_double(beta), _p(u), _p(mom), _p(loc))
+        return loc
+
     # force ---------------------------------------------------------------
     def fermion_force_begin(self):
         self.L.orc_fermion_force_begin()

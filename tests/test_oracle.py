@@ -312,3 +312,76 @@ def test_mre_guess_formula():
     g = o.mre_guess(O.OP_DPHI_EOPRE, sols, pf)
     ref = _mre_numpy(o, lambda s: o.Dphi_eopre(0.1, s), sols, pf)
     assert np.abs(g - ref).max() / np.abs(ref).max() < 1e-12
+
+
+# ---- HMC pieces (LibHR/Update/force0.c, field_update.c, local_action.c, suN_utils.c)
+def _perturb(o, u, w, eps):
+    gT = o.generators()[0]
+    X = np.einsum("xma,aij->xmij", eps * w, gT)
+    E = F.exp_i_hermitian(X.reshape(-1, o.ng, o.ng)).reshape(u.shape)
+    return np.einsum("xmij,xmjk->xmik", E, u)
+
+
+@pytest.mark.parametrize("ng", [2, 3])
+def test_force0_is_minus_twice_gauge_action_derivative(ng):
+    o = O.Oracle(4, 4, 4, 4, ng, O.FUND)
+    u = F.smooth_gauge(4, o.V, ng, 0.4)
+    beta = 2.25
+    dimg = ng * ng - 1
+    zero = np.zeros((o.V, 4, dimg))
+    f = o.force0(1.0, beta, u, zero)
+    w = np.random.default_rng(5).standard_normal((o.V, 4, dimg))
+    S = lambda uu: o.local_hmc_action(beta, uu, zero).sum()
+    eps = 1e-5
+    fd = (S(_perturb(o, u, w, eps)) - S(_perturb(o, u, w, -eps))) / (2 * eps)
+    an = -0.5 * np.sum(w * f)
+    assert abs(fd - an) < 1e-7 * abs(an)
+
+
+def test_update_exponential_and_projection():
+    o = O.Oracle(4, 4, 4, 4, 3, O.FUND)
+    u = F.smooth_gauge(6, o.V, 3, 0.3)
+    mom = np.random.default_rng(7).standard_normal((o.V, 4, 8))
+    dt = 0.05
+    u2 = o.update_gauge_field(dt, u, mom)
+    gT = o.generators()[0]
+    X = np.einsum("xma,aij->xmij", dt * mom, gT)
+    ref = np.einsum("xmij,xmjk->xmik", F.exp_i_hermitian(X.reshape(-1, 3, 3)).reshape(u.shape), u)
+    assert np.abs(u2 - ref).max() < 1e-14
+    # projection: SU(3) result, the identity on SU(3) input, a fix of a perturbed link
+    p = o.project_gauge_field(u2)
+    assert np.abs(p - u2).max() < 1e-13
+    noisy = u2 + 1e-3 * np.random.default_rng(8).standard_normal(u2.shape)
+    q = o.project_gauge_field(noisy).reshape(-1, 3, 3)
+    assert np.abs(np.einsum("kij,klj->kil", q, q.conj()) - np.eye(3)).max() < 1e-14
+    assert np.abs(np.linalg.det(q) - 1).max() < 1e-14
+
+
+def test_local_action_is_momenta_plus_plaquette_action():
+    o = O.Oracle(4, 4, 4, 4, 2, O.FUND)
+    u = F.smooth_gauge(9, o.V, 2, 0.5)
+    mom = np.random.default_rng(10).standard_normal((o.V, 4, 3))
+    beta = 2.25
+    loc = o.local_hmc_action(beta, u, mom)
+    expect = 0.25 * np.sum(mom * mom) - beta / 2 * 6 * 2 * o.V * o.avr_plaquette(u)
+    assert abs(loc.sum() - expect) < 1e-9 * abs(expect)
+
+
+def test_pure_gauge_leapfrog_energy_violation_scales_as_dt_squared():
+    o = O.Oracle(4, 4, 4, 4, 2, O.FUND)
+    u0 = F.smooth_gauge(11, o.V, 2, 0.4)
+    p0 = np.random.default_rng(12).standard_normal((o.V, 4, 3))
+    beta, tau = 2.25, 0.5
+
+    def dH(nsteps):
+        dt = tau / nsteps
+        u, p = u0.copy(), p0.copy()
+        H0 = o.local_hmc_action(beta, u, p).sum()
+        p = o.force0(dt / 2, beta, u, p)
+        for s in range(nsteps):
+            u = o.update_gauge_field(dt, u, p)
+            p = o.force0(dt if s < nsteps - 1 else dt / 2, beta, u, p)
+        return o.local_hmc_action(beta, u, p).sum() - H0
+
+    d1, d2 = dH(10), dH(20)
+    assert 3.5 < d1 / d2 < 4.5, (d1, d2)  # leapfrog: dH = O(dt^2)
