@@ -24,7 +24,12 @@ def haar_su_n(rng, count, n):
 
 
 def exp_i_hermitian(h):
-    """exp(i h) for a stack of Hermitian matrices, by eigendecomposition."""
+    """exp(i h) for a stack of Hermitian matrices, by eigendecomposition (2x2
+    traceless: cos|a| + i sin|a| h/|a|, |a|^2 = -det h)."""
+    if h.shape[-1] == 2 and np.allclose(h[..., 0, 0] + h[..., 1, 1], 0.0, atol=1e-14):
+        a = np.sqrt(np.maximum(-np.linalg.det(h).real, 0.0))[..., None, None]
+        sinc = np.where(a > 0, np.sin(a) / np.where(a > 0, a, 1.0), 1.0)
+        return np.cos(a) * np.eye(2) + 1j * sinc * h
     w, v = np.linalg.eigh(h)
     return np.einsum("...ij,...j,...kj->...ik", v, np.exp(1j * w), v.conj())
 

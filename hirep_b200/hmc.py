@@ -1,0 +1,137 @@
+"""One HMC trajectory on the GPU, driven from the host as HiRep drives it.
+
+update_ghmc (LibHR/Update/update_mt.c:148-260) with two monomials: the
+plaquette gauge action (mon_pg.c; force0.c) and an Nf = 2 Wilson pseudofermion
+on the even sites (mon_hmc.c; force_hmc.c, UPDATE_EO branch), integrated with
+the second-order Omelyan integrator (integrators.c:64-93, lambda =
+0.1931833275037836).  Links, momenta and pseudofermions stay on the device; the
+host only holds the scalars of the recursion and the random numbers.
+
+The force solves are either HiRep's (two g5QMR solves on D) or, as the
+mixed-precision form of this library, one CG on H^2 = (g5 D)^2 (FP64 or FP32
+inner defect correction): Ys = (H^2)^-1 pf and Xs = H Ys, the pair that
+force_fermion_core expects (for g5QMR: Xs = H^-1 pf, Ys = H^-1 Xs).
+"""
+import time
+
+import numpy as np
+
+from . import hrgpu as G
+
+LAMBDA_O2MN = 0.1931833275037836
+
+
+class HMC:
+    def __init__(self, lat, beta, mass, tau, nsteps, force_err2=1e-20, mt_err2=1e-28, force_solver="cg_mixed",
+                 bc_t_antiperiodic=True):
+        if lat.csw is not None:
+            # the clover monomial also needs force_clover_logdet and clover_la_logdet
+            raise NotImplementedError("HMC driver: Wilson fermions only (no clover log-det terms)")
+        if force_solver not in ("cg_mixed", "cg", "g5qmr"):
+            raise ValueError("force_solver: cg_mixed, cg or g5qmr")
+        self.lat, self.beta, self.mass, self.tau, self.nsteps = lat, beta, mass, tau, nsteps
+        self.force_err2, self.mt_err2, self.force_solver = force_err2, mt_err2, force_solver
+        self.bc = bc_t_antiperiodic
+        E = G.EVEN
+        self.pf, self.x, self.y, self.tmp = (lat.field(E) for _ in range(4))
+        self.Xs, self.Ys = lat.field(G.FULL), lat.field(G.FULL)
+        self.iters = 0
+        self.nforce = 0
+
+    # -- monomial pieces ----------------------------------------------------------
+    def _even_into_full(self, full, even):
+        full.buf[: even.nbytes].copy_(even.buf)
+        full.buf[even.nbytes:].zero_()
+
+    def _solve(self, op, out, src, err2, flt):
+        it, ok = self.lat.cg_mshift(op, self.mass, [0.0], err2, src, [out], flt=flt)
+        self.iters += it
+        if not ok:
+            raise G.HRGPUError("HMC: force solve did not converge")
+
+    def fermion_force(self, dt):
+        """force_hmc (force_hmc.c:58-195) for the Nf = 2 Wilson monomial, UPDATE_EO."""
+        lat = self.lat
+        if self.force_solver == "g5qmr":
+            # X = H^-1 pf = D^-1 g5 pf, Y = H^-1 X = D^-1 g5 X
+            lat.la("g5", self.tmp, self.pf)
+            lat.la("zero", self.x)
+            it, ok = lat.g5QMR_mshift(G.OP_DPHI_EOPRE, self.mass, [0.0], self.force_err2, self.tmp, [self.x])
+            lat.la("g5", self.tmp, self.x)
+            lat.la("zero", self.y)
+            it2, ok2 = lat.g5QMR_mshift(G.OP_DPHI_EOPRE, self.mass, [0.0], self.force_err2, self.tmp, [self.y])
+            self.iters += it + it2
+            if not (ok and ok2):
+                raise G.HRGPUError("HMC: g5QMR force solve did not converge")
+            X, Y = self.x, self.y
+        else:
+            # Y = (H^2)^-1 pf (start from the previous solution), X = H Y
+            self._solve(G.OP_G5DPHI_EOPRE_SQ, self.y, self.pf, self.force_err2, self.force_solver == "cg_mixed")
+            lat.g5Dphi_eopre(self.mass, self.x, self.y)
+            X, Y = self.x, self.y
+        self._even_into_full(self.Xs, X)
+        self._even_into_full(self.Ys, Y)
+        lat.fermion_force_begin()
+        lat.force_fermion_core(self.Xs, self.Ys, 1, dt, 1.0)
+        lat.fermion_force_end_momenta(dt)
+        self.nforce += 1
+
+    def force(self, dt):
+        """monomial_force (integrators.c:12-19): every monomial's force."""
+        self.lat.force0(dt, self.beta)
+        self.fermion_force(dt)
+
+    def field(self, dt):
+        """monomial_field: the gauge monomial's update_gauge_field."""
+        self.lat.update_gauge_field(dt)
+
+    def o2mn(self):
+        """O2MN_multistep (integrators.c:64-93)."""
+        dt = self.tau / self.nsteps
+        lam = LAMBDA_O2MN
+        for n in range(self.nsteps):
+            self.force(lam * dt if n == 0 else 2 * lam * dt)
+            self.field(dt / 2)
+            self.force((1 - 2 * lam) * dt)
+            self.field(dt / 2)
+        self.force(lam * dt)
+
+    # -- one trajectory -------------------------------------------------------------
+    def trajectory(self, rng, metropolis=True):
+        """update_ghmc: returns dH, acceptance and timings.  rng: numpy Generator."""
+        lat = self.lat
+        lat.set_dirac_mass(self.mass)
+        u_old = lat.gauge_get()
+        t0 = time.perf_counter()
+        # momenta (random_momenta.c: gauss / sqrt(C(F))) and pseudofermion heatbath
+        # (gaussian_spinor_field: gauss / sqrt(2)); the starting action holds |eta|^2
+        lat.momenta_set(rng.standard_normal((lat.V, 4, lat.dimg)) / np.sqrt(0.5))
+        eta_h = (rng.standard_normal((lat.VH, 4, lat.nf)) + 1j * rng.standard_normal((lat.VH, 4, lat.nf))) / np.sqrt(2)
+        eta = lat.field(G.EVEN, host=eta_h)
+        lat.local_hmc_action(False, self.beta)
+        lat.pf_local_action(eta)
+        lat.g5Dphi_eopre(self.mass, self.pf, eta)  # correct_pf: pf = H eta
+        lat.la("zero", self.y)
+        self.iters = 0
+        self.nforce = 0
+        self.o2mn()
+        lat.project_gauge_field()
+        lat.represent_gauge_field(self.bc)
+        # correct_la_pf: pf <- H^-1 pf = D^-1 g5 pf (g5QMR, FP64, MT precision)
+        lat.la("g5", self.tmp, self.pf)
+        lat.la("zero", self.pf)
+        it, ok = lat.g5QMR_mshift(G.OP_DPHI_EOPRE, self.mass, [0.0], self.mt_err2, self.tmp, [self.pf])
+        if not ok:
+            raise G.HRGPUError("HMC: accept/reject solve did not converge")
+        lat.local_hmc_action(True, self.beta)
+        lat.pf_local_action(self.pf)
+        dH = lat.local_action_sum()
+        lat.sync()
+        t1 = time.perf_counter()
+        accepted = True
+        if metropolis and dH > 0 and rng.uniform() >= np.exp(-dH):
+            accepted = False
+            lat.set_gauge(u_old)
+            lat.represent_gauge_field(self.bc)
+        return {"dH": dH, "accepted": accepted, "seconds": t1 - t0, "force_solve_iters": self.iters,
+                "force_evaluations": self.nforce, "mt_iters": it}

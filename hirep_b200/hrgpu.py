@@ -157,6 +157,7 @@ class Lattice:
         self.nf = self.L.hrgpu_nf()
         self.real = repr_ == ADJ
         self.dimg = ng * ng - 1
+        self.csw = None  # clover coefficient once clover_init was called
 
     def nsites(self, par):
         return self.V if par == FULL else self.VH
@@ -226,6 +227,7 @@ class Lattice:
     # clover --------------------------------------------------------------
     def clover_init(self, csw):
         _check(self.L.hrgpu_clover_init(D(csw)), "clover_init")
+        self.csw = csw
 
     def compute_clover_term(self):
         _check(self.L.hrgpu_compute_clover_term(), "compute_clover_term")
