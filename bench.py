@@ -183,6 +183,7 @@ def main():
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 22-system solve (24^3x48 sextet)")
     ap.add_argument("--no-force", action="store_true", help="skip the force check (16^4 SU(4) antisymmetric)")
+    ap.add_argument("--no-hmc", action="store_true", help="skip the HMC trajectory (32^3x64 SU(2) adjoint)")
     ap.add_argument("--batch-op", default=None, metavar="TxXxYxZ",
                     help="only time the batched g5Cphi_eopre of the batched workload on this lattice")
     ap.add_argument("--nb", type=int, default=12, help="fields per batch for --batch-op")
@@ -301,6 +302,8 @@ def main():
         line["solve_batch"] = run_batch_solves(torch, stream, G, F)
     if world == 1 and not args.no_force:
         line["force"] = run_force_check(torch, stream, G, F)
+    if world == 1 and not args.no_hmc:
+        line["hmc"] = run_hmc_check(torch, G, F)
     if rank == 0 and world == 1 and not args.no_cpu:
         base, _ = cpu_reference_arm(args)
         line["cpu_baseline"] = base
@@ -467,6 +470,36 @@ def run_force_check(torch, stream, G, F, ndir=4, step=1e-3):
             "fd": f"{ndir} random su(4) directions on all links, 4th-order central differences, step {step}",
             "fd_max_rel_err_fp64": worst,
             "mixed_vs_fp64_force_rel_err": float(np.abs(f32 - f64).max() / np.abs(f64).max())}
+
+
+# HMC workload: SU(2) adjoint (NF = 3, real), Nf = 2 Wilson m0 = -1.0, plaquette
+# action beta = 2.25, 32^3 x 64, U = exp(i 0.2 H) seed 99; one trajectory of length 1,
+# O2MN with 20 steps; force solves at |r|/|b| < 1e-10, accept/reject at 1e-14
+H_DIMS, H_NG, H_BETA, H_MASS, H_EPS, H_SEED = (64, 32, 32, 32), 2, 2.25, -1.0, 0.2, 99
+
+
+def run_hmc_check(torch, G, F):
+    """One trajectory with mixed-precision force solves against the same trajectory
+    (same random numbers) with plain FP64 force solves."""
+    from hirep_b200.hmc import HMC
+
+    lat = G.Lattice(*H_DIMS, H_NG, G.ADJ)
+    u0 = F.smooth_gauge(H_SEED, lat.V, H_NG, H_EPS)
+    out = {"workload": "SU(2) adjoint Nf=2 Wilson m0=-1.0 + plaquette beta=2.25, 32^3x64, U=exp(i0.2H) seed 99; "
+                       "O2MN tau=1, 20 steps; force solves 1e-10, accept/reject 1e-14"}
+    for name, solver in (("mixed", "cg_mixed"), ("fp64", "cg")):
+        lat.set_gauge(u0)
+        lat.represent_gauge_field(True)
+        plaq0 = lat.avr_plaquette()
+        hmc = HMC(lat, H_BETA, H_MASS, tau=1.0, nsteps=20, force_err2=1e-20, mt_err2=1e-28, force_solver=solver)
+        torch.cuda.synchronize()
+        r = hmc.trajectory(np.random.default_rng(H_SEED), metropolis=False)
+        out[name] = {"seconds": r["seconds"], "dH": r["dH"], "force_solve_mvm": r["force_solve_iters"],
+                     "force_evaluations": r["force_evaluations"], "accept_reject_mvm": r["mt_iters"],
+                     "plaquette_start": plaq0, "plaquette_end": lat.avr_plaquette()}
+    out["speedup_mixed_vs_fp64"] = out["fp64"]["seconds"] / out["mixed"]["seconds"]
+    out["dH_difference"] = out["mixed"]["dH"] - out["fp64"]["dH"]
+    return out
 
 
 def batch_op_main(args, torch, G, F):

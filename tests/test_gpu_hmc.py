@@ -182,3 +182,20 @@ def test_hmc_force_solver_forms_agree(solver):
         hmc = HMC(lat, beta, mass, tau=0.5, nsteps=10, force_err2=1e-24, force_solver=s)
         out[s] = hmc.trajectory(np.random.default_rng(6), metropolis=False)["dH"]
     assert abs(out[solver] - out["cg"]) < 1e-7 * max(1.0, abs(out["cg"]))
+
+
+def test_hmc_energy_violation_scales_as_dt_squared():
+    """Full system (plaquette + Nf=2 Wilson): O2MN's dH falls as dt^2, so the
+    forces, the momenta's kinetic term and the actions are consistent."""
+    from hirep_b200.hmc import HMC
+
+    dims, ng, beta, mass = (4, 4, 4, 4), 2, 2.25, -1.0
+    u0 = F.smooth_gauge(7, 256, ng, 0.3)
+    dh = {}
+    for n in (16, 32):
+        lat = G.Lattice(*dims, ng, G.ADJ)
+        lat.set_gauge(u0)
+        lat.represent_gauge_field(True)
+        hmc = HMC(lat, beta, mass, tau=0.5, nsteps=n, force_err2=1e-26, force_solver="cg")
+        dh[n] = hmc.trajectory(np.random.default_rng(8), metropolis=False)["dH"]
+    assert 3.5 < dh[16] / dh[32] < 4.5, dh  # the oracle trajectory gives 3.97 here
