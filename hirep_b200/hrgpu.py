@@ -372,6 +372,16 @@ class Lattice:
         _check(self.L.hrgpu_avr_plaquette(ctypes.byref(p)), "avr_plaquette")
         return p.value
 
+    def write_gauge_field(self, filename):
+        _check(self.L.hrgpu_write_gauge_field(str(filename).encode()), "write_gauge_field")
+
+    def read_gauge_field(self, filename):
+        """Returns (plaquette stored in the file, plaquette of the links read)."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _check(self.L.hrgpu_read_gauge_field(str(filename).encode(), ctypes.byref(a), ctypes.byref(b)),
+               "read_gauge_field")
+        return a.value, b.value
+
     def fermion_force_end_momenta(self, dt):
         _check(self.L.hrgpu_fermion_force_end_momenta(D(dt)), "fermion_force_end_momenta")
 

@@ -289,6 +289,17 @@ int hrgpu_avr_plaquette(double *plaq);
 /* fermion_force_end (force_fermion_core.c:964-993) adding into the device momenta */
 int hrgpu_fermion_force_end_momenta(double dt);
 
+/* ------------------------------------------------------------- gauge IO -- */
+/* write_gauge_field / read_gauge_field (LibHR/IO/archive.c:26-457,
+ * archive_su2quat.c): HiRep's big-endian file (NG, T, X, Y, Z, the average
+ * plaquette, then the links of each site in (t, x, y, z) order, z fastest; SU(2)
+ * as quaternions, read in either form) to and from the device's fundamental
+ * links.  The reader refuses another NG or lattice size and reports the stored
+ * and the recomputed plaquette (the reference warns when they differ by more
+ * than 1e-12); call hrgpu_represent_gauge_field afterwards. */
+int hrgpu_write_gauge_field(const char *filename);
+int hrgpu_read_gauge_field(const char *filename, double *plaq_file, double *plaq_read);
+
 /* ------------------------------------------------------ batched (multi-RHS) -- */
 /* HiRep has no batched interface; these entry points serve its callers that
  * hold many sources at once (calc_prop.c:210-289 loops cg_mshift over the 4*NF
