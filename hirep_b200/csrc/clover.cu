@@ -113,25 +113,6 @@ __global__ void k_clover_term(double2 *cl, const void *U, Geo g, double csw) {
     }
 }
 
-// Hermitian block b (0: s0,s1; 1: s2,s3) plus sigma on the diagonal, element (i,j), i >= j
-template <int N>
-__device__ __forceinline__ double2 hblock(const double2 *cl, int b, int i, int j, long lp, long d, double sigma) {
-  const int N2 = N * N;
-  const double2 *sa = cl + (long)(2 * b) * N2 * lp + d, *sb = cl + (long)(2 * b + 1) * N2 * lp + d;
-  double2 v;
-  if (i < N) {
-    v = __ldg(sa + (long)(i * N + j) * lp);
-  } else if (j < N) {
-    double2 s = __ldg(sb + (long)(j * N + (i - N)) * lp);
-    v = make_double2(s.x, -s.y);
-  } else {
-    double2 s = __ldg(sa + (long)((i - N) * N + (j - N)) * lp);
-    v = make_double2(-s.x, -s.y);
-  }
-  if (i == j) v.x += sigma;
-  return v;
-}
-
 template <int N>
 __global__ void k_clover_pack_diag(const double2 *cl, double sigma, double *dg, double2 *od, Geo g) {
   long d = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -206,6 +187,81 @@ __global__ void k_clover_pack_inv(const double2 *cl, double sigma, double *dg, d
 #undef CP
 }
 
+// exponential clover (Dphi.c:1292-1482, LibHR/Utils/clover_exp.c): per chiral
+// block A, D = sigma exp(A / sigma) and D^-1 = exp(-A / sigma) / sigma, both
+// Hermitian and packed like the blocks above.  The exponential is scaling and
+// squaring of the Taylor series to order 20 in FP64 (the reference's series are
+// exact to rounding as well).  One block of (2NF)^2 threads per site, one
+// matrix element per thread, the matrices in shared memory (this runs once per
+// mass).
+template <int N>
+__global__ void __launch_bounds__(4 * N * N) k_clover_pack_exp(const double2 *cl, double sigma, double *dg, double2 *od, double *idg, double2 *iod,
+                                  Geo g) {
+  constexpr int n = 2 * N, NO = N * (2 * N - 1);
+  __shared__ double2 A[n * n], T[n * n], E[n * n];
+  __shared__ int s_sq;
+  const long d = blockIdx.x;
+  const int p = d >= g.ld ? 1 : 0;
+  const long lp = 2L * g.ld;
+  const int t = threadIdx.x, i = t / n, j = t % n;
+  if (d - p * g.ld >= g.VH) {  // padding sites
+    for (int b = 0; b < 2; b++) {
+      if (i == j) dg[((long)b * n + i) * lp + d] = idg[((long)b * n + i) * lp + d] = 0.0;
+      if (i > j) {
+        const long k = ((long)b * NO + i * (i - 1) / 2 + j) * lp + d;
+        od[k] = iod[k] = make_double2(0, 0);
+      }
+    }
+    return;
+  }
+  for (int b = 0; b < 2; b++)
+    for (int sgn = 0; sgn < 2; sgn++) {
+      const double c = (sgn ? -1.0 : 1.0) / sigma;
+      double2 v = (i >= j) ? hblock<N>(cl, b, i, j, lp, d, 0.0) : hblock<N>(cl, b, j, i, lp, d, 0.0);
+      if (i < j) v.y = -v.y;
+      A[t] = make_double2(c * v.x, c * v.y);
+      __syncthreads();
+      if (t == 0) {
+        double nrm = 0;
+        for (int k = 0; k < n * n; k++) nrm += A[k].x * A[k].x + A[k].y * A[k].y;
+        nrm = sqrt(nrm);
+        int sq = 0;
+        while (nrm > 0.25 && sq < 60) {
+          nrm *= 0.5;
+          sq++;
+        }
+        s_sq = sq;
+      }
+      __syncthreads();
+      const int sq = s_sq;
+      const double sc = ldexp(1.0, -sq);
+      A[t] = make_double2(A[t].x * sc, A[t].y * sc);
+      E[t] = T[t] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+      __syncthreads();
+      for (int k = 1; k <= 20; k++) {  // T <- T A / k, E += T
+        double2 acc = make_double2(0, 0);
+        for (int l = 0; l < n; l++) cmac(acc, T[i * n + l], A[l * n + j]);
+        __syncthreads();
+        T[t] = make_double2(acc.x / k, acc.y / k);
+        E[t] = cadd(E[t], T[t]);
+        __syncthreads();
+      }
+      for (int q = 0; q < sq; q++) {  // E <- E E
+        double2 acc = make_double2(0, 0);
+        for (int l = 0; l < n; l++) cmac(acc, E[i * n + l], E[l * n + j]);
+        __syncthreads();
+        E[t] = acc;
+        __syncthreads();
+      }
+      const double scale = sgn ? 1.0 / sigma : sigma;
+      double *pdg = sgn ? idg : dg;
+      double2 *pod = sgn ? iod : od;
+      if (i == j) pdg[((long)b * n + i) * lp + d] = scale * E[t].x;
+      if (i > j) pod[((long)b * NO + i * (i - 1) / 2 + j) * lp + d] = make_double2(scale * E[t].x, scale * E[t].y);
+      __syncthreads();
+    }
+}
+
 template <typename DST, typename SRC>
 __global__ void k_cvt(DST *dst, const SRC *src, long n) {
   long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -274,6 +330,12 @@ int clover_prepare(double mass, int prec) {
   Geo g = make_geo();
   long n = 2L * L.ld;
   const long lp = 2L * L.ld;
+  if (L.expclover && (L.sigma_diag != sigma || L.sigma != sigma)) {
+    HR_NFC_DISPATCH(L.nf, (k_clover_pack_exp<N_><<<(unsigned)n, 4 * N_ * N_, 0, L.stream>>>(L.cl_term, sigma, L.cl_dg, L.cl_od, L.cl_idg, L.cl_iod, g)));
+    HR_LAUNCH_CHECK();
+    L.sigma_diag = L.sigma = sigma;
+    L.clover_gen[HRGPU_DOUBLE]++;
+  }
   if (L.sigma_diag != sigma) {
     HR_NFC_DISPATCH(L.nf, (k_clover_pack_diag<N_><<<nb(n), 128, 0, L.stream>>>(L.cl_term, sigma, L.cl_dg, L.cl_od, g)));
     HR_LAUNCH_CHECK();
@@ -337,9 +399,16 @@ int hrgpu_clover_init(double csw) {
   HR_REQUIRE(L.ready, HRGPU_E_STATE, "hrgpu_clover_init: lattice not initialised");
   if (int rc = alloc_clover()) return rc;
   L.clover = true;
+  L.expclover = false;
   L.csw = csw;
   L.sigma = L.sigma_diag = L.sigma_flt = 0xF00F;
   if (L.have_gauge) return compute_clover_term_dev();
+  return 0;
+}
+
+int hrgpu_expclover_init(double csw) {
+  if (int rc = hrgpu_clover_init(csw)) return rc;
+  L.expclover = true;
   return 0;
 }
 

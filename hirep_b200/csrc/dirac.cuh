@@ -132,4 +132,57 @@ __device__ __forceinline__ void madd(CMat<N> &A, const CMat<N> &B) {
   for (int k = 0; k < N * N; k++) A.c[k] = cadd(A.c[k], B.c[k]);
 }
 
+// Hermitian clover block b (0: s0,s1; 1: s2,s3) of the clover term in its
+// device planes [4][NF*NF][2ld], plus sigma on the diagonal, element (i,j), i >= j
+template <int N>
+__device__ __forceinline__ double2 hblock(const double2 *cl, int b, int i, int j, long lp, long d, double sigma) {
+  const int N2 = N * N;
+  const double2 *sa = cl + (long)(2 * b) * N2 * lp + d, *sb = cl + (long)(2 * b + 1) * N2 * lp + d;
+  double2 v;
+  if (i < N) {
+    v = __ldg(sa + (long)(i * N + j) * lp);
+  } else if (j < N) {
+    double2 s = __ldg(sb + (long)(j * N + (i - N)) * lp);
+    v = make_double2(s.x, -s.y);
+  } else {
+    double2 s = __ldg(sa + (long)((i - N) * N + (j - N)) * lp);
+    v = make_double2(-s.x, -s.y);
+  }
+  if (i == j) v.x += sigma;
+  return v;
+}
+
+// e = exp(x) of an N x N complex matrix: scaling and squaring of the Taylor
+// series to order 20 (the norm is scaled below 1/4 first), exact to rounding
+template <int N>
+__device__ void mexp_sq(CMat<N> &e, const CMat<N> &x) {
+  double nrm = 0;
+  for (int k = 0; k < N * N; k++) nrm += x.c[k].x * x.c[k].x + x.c[k].y * x.c[k].y;
+  nrm = sqrt(nrm);
+  int sq = 0;
+  while (nrm > 0.25 && sq < 60) {
+    nrm *= 0.5;
+    sq++;
+  }
+  const double scale = ldexp(1.0, -sq);
+  CMat<N> a, term, tmp;
+  for (int k = 0; k < N * N; k++) {
+    a.c[k] = make_double2(x.c[k].x * scale, x.c[k].y * scale);
+    e.c[k] = make_double2((k % (N + 1) == 0) ? 1.0 : 0.0, 0.0);
+    term.c[k] = e.c[k];
+  }
+  for (int j = 1; j <= 20; j++) {
+    mmul<N, false, false>(tmp, term, a);
+    const double inv = 1.0 / j;
+    for (int k = 0; k < N * N; k++) {
+      term.c[k] = make_double2(tmp.c[k].x * inv, tmp.c[k].y * inv);
+      e.c[k] = cadd(e.c[k], term.c[k]);
+    }
+  }
+  for (int q = 0; q < sq; q++) {
+    mmul<N, false, false>(tmp, e, e);
+    e = tmp;
+  }
+}
+
 }  // namespace hrgpu

@@ -145,6 +145,132 @@ __global__ void k_force_clover_fermion(double2 *clf, const double2 *X, const dou
     }
 }
 
+// The exponential clover's force matrices (force_fermion_core.c:484-772).  With
+// D = (4+m) exp(Ah), Ah = A/(4+m) on each chirality block, the derivative of
+// the block along dA is the Frechet derivative of the exponential,
+//   L(Ah, dA) = sum_{k,l} Ah^k dA Ah^l / (k+l+1)! ,
+// which the reference expands in powers of Ah (its Taylor or Cayley-Hamilton
+// coefficients C_kl).  Contracted with the fields it turns Y X^+, the matrix of
+// the linear term's sigma insertions, into P = L(Ah, Y X^+) per block.  Here P
+// is computed by scaling and squaring instead of a power expansion: with Ah and
+// E = Y X^+ scaled by 2^-s (|Ah|_F <= 1/4), the Taylor recursions
+//   T_k = T_{k-1} Ah / k ,  S_k = (T_{k-1} E + S_{k-1} Ah) / k      (k <= 16)
+// sum to e = exp(Ah) and P = L(Ah, E), then s doublings P <- e P + P e,
+// e <- e e.  One block of (2NF)^2 threads per site, one matrix element each,
+// seven 2NF x 2NF matrices in dynamic shared memory.
+constexpr int EXPF_TAYLOR = 16;
+// g5 sigma_{mu nu} for the six (mu,nu) of cl_force: component c of the result is
+// (fr + i fi) times component src of the input (the tables of g5_sigma above)
+__constant__ int c_sig_src[6][4] = {{1, 0, 3, 2}, {1, 0, 3, 2}, {0, 1, 2, 3}, {0, 1, 2, 3}, {1, 0, 3, 2}, {1, 0, 3, 2}};
+__constant__ double c_sig_fr[6][4] = {{0, 0, 0, 0}, {-1, 1, -1, 1}, {0, 0, 0, 0}, {0, 0, 0, 0}, {-1, 1, 1, -1}, {0, 0, 0, 0}};
+__constant__ double c_sig_fi[6][4] = {{-1, -1, -1, -1}, {0, 0, 0, 0}, {1, -1, -1, 1}, {-1, 1, -1, 1}, {0, 0, 0, 0}, {1, 1, -1, -1}};
+template <int N>
+constexpr size_t expf_smem() { return sizeof(double2) * 7 * (2 * N) * (2 * N); }
+
+template <int N, bool REAL>
+__global__ void __launch_bounds__(4 * N * N) k_force_expclover_fermion(double2 *clf, const double2 *cl, const double2 *X,
+                                                                       const double2 *Y, Geo g, double sigma,
+                                                                       double residue) {
+  constexpr int n = 2 * N, nn = n * n;
+  extern __shared__ double2 sm[];
+  double2 *A = sm, *E = sm + nn, *T = sm + 2 * nn, *S = sm + 3 * nn, *Ex = sm + 4 * nn, *P0 = sm + 5 * nn,
+          *P1 = sm + 6 * nn;
+  __shared__ int s_sq;
+  const long d = blockIdx.x;
+  const int p = d >= g.ld ? 1 : 0;
+  if (d - p * g.ld >= g.VH) return;  // padding site: the whole block leaves
+  const long lp = 2L * g.ld;
+  const int t = threadIdx.x, i = t / n, j = t % n;
+  for (int b = 0; b < 2; b++) {
+    double2 *P = b ? P1 : P0;
+    double2 v = (i >= j) ? hblock<N>(cl, b, i, j, lp, d, 0.0) : hblock<N>(cl, b, j, i, lp, d, 0.0);
+    if (i < j) v.y = -v.y;
+    A[t] = make_double2(v.x / sigma, v.y / sigma);
+    const double2 yi = *sp_at(Y, d, 2 * b * N + i, g.ld, N), xj = *sp_at(X, d, 2 * b * N + j, g.ld, N);
+    E[t] = make_double2(yi.x * xj.x + yi.y * xj.y, yi.y * xj.x - yi.x * xj.y);  // y_i conj(x_j)
+    __syncthreads();
+    if (t == 0) {
+      double nrm = 0;
+      for (int k = 0; k < nn; k++) nrm += A[k].x * A[k].x + A[k].y * A[k].y;
+      nrm = sqrt(nrm);
+      int sq = 0;
+      while (nrm > 0.25 && sq < 60) {
+        nrm *= 0.5;
+        sq++;
+      }
+      s_sq = sq;
+    }
+    __syncthreads();
+    const int sq = s_sq;
+    const double sc = ldexp(1.0, -sq);
+    A[t] = make_double2(A[t].x * sc, A[t].y * sc);
+    E[t] = make_double2(E[t].x * sc, E[t].y * sc);
+    T[t] = Ex[t] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+    S[t] = P[t] = make_double2(0, 0);
+    __syncthreads();
+    for (int k = 1; k <= EXPF_TAYLOR; k++) {
+      double2 ta = make_double2(0, 0), sa = make_double2(0, 0);
+      for (int l = 0; l < n; l++) {
+        const double2 tl = T[i * n + l];
+        cmac(ta, tl, A[l * n + j]);
+        cmac(sa, tl, E[l * n + j]);
+        cmac(sa, S[i * n + l], A[l * n + j]);
+      }
+      __syncthreads();
+      T[t] = make_double2(ta.x / k, ta.y / k);
+      S[t] = make_double2(sa.x / k, sa.y / k);
+      Ex[t] = cadd(Ex[t], T[t]);
+      P[t] = cadd(P[t], S[t]);
+      __syncthreads();
+    }
+    for (int q = 0; q < sq; q++) {
+      double2 ea = make_double2(0, 0), pa = make_double2(0, 0);
+      for (int l = 0; l < n; l++) {
+        const double2 el = Ex[i * n + l];
+        cmac(ea, el, Ex[l * n + j]);
+        cmac(pa, el, P[l * n + j]);
+        cmac(pa, P[i * n + l], Ex[l * n + j]);
+      }
+      __syncthreads();
+      Ex[t] = ea;
+      P[t] = pa;
+      __syncthreads();
+    }
+  }
+  // the sigma insertions of the linear term (g5_sigma, fmat_create) with P in
+  // place of Y X^+: sum_c f_qc (P[(s_c,i),(c,j)] + conj(P[(c,j),(s_c,i)]))
+  for (int o = t; o < 6 * N * N; o += blockDim.x) {
+    const int q = o / (N * N), ii = (o / N) % N, jj = o % N;
+    double2 s = make_double2(0, 0);
+    for (int c = 0; c < 4; c++) {
+      const int sc = c_sig_src[q][c];
+      const double2 *P = (c >> 1) ? P1 : P0;
+      const double2 a = P[((sc & 1) * N + ii) * n + (c & 1) * N + jj];
+      const double2 bb = P[((c & 1) * N + jj) * n + (sc & 1) * N + ii];
+      const double2 w = make_double2(a.x + bb.x, a.y - bb.y);
+      s.x += c_sig_fr[q][c] * w.x - c_sig_fi[q][c] * w.y;
+      s.y += c_sig_fr[q][c] * w.y + c_sig_fi[q][c] * w.x;
+    }
+    if (REAL) s.y = 0.0;
+    double2 &out = clf[((long)q * N * N + ii * N + jj) * lp + d];
+    out.x += residue * s.x;
+    out.y += residue * s.y;
+  }
+}
+
+template <int N, bool REAL>
+static int launch_force_expclover(double2 *clf, const double2 *cl, const double2 *X, const double2 *Y, Geo g,
+                                  double sigma, double residue) {
+  constexpr size_t smem = expf_smem<N>();
+  if (smem > 48 * 1024)
+    HR_CUDA(cudaFuncSetAttribute(k_force_expclover_fermion<N, REAL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  k_force_expclover_fermion<N, REAL><<<(unsigned)(2L * g.ld), 4 * N * N, smem, L.stream>>>(clf, cl, X, Y, g, sigma,
+                                                                                          residue);
+  HR_LAUNCH_CHECK();
+  return 0;
+}
+
 // force_clover_core (force_fermion_core.c:282-379): one thread per (site, mu)
 template <int N, bool REAL>
 __global__ void k_force_clover_core(double *fsum, const void *U, const double2 *clf, Geo g, ProjTab P, double coeff) {
@@ -357,7 +483,9 @@ int hrgpu_force_fermion_core(void *Xs, void *Ys, int auto_fill_odd, double dt, d
   const double coeff = -residue * dt * (L.repr_norm2 / L.fund_norm2);
   Geo g = make_geo();
   const long n = 2L * L.ld;
-  if (L.clover) {
+  if (L.clover && L.expclover) {
+    HR_NF_DISPATCH(L.real, L.nf, (launch_force_expclover<N_, R_>(L.cl_force, L.cl_term, X, Y, g, 4.0 + static_mass(), residue)));
+  } else if (L.clover) {
     HR_NF_DISPATCH(L.real, L.nf, (k_force_clover_fermion<N_, R_><<<dim3(nb(n), 6), 128, 0, L.stream>>>(L.cl_force, X, Y, g, residue)));
     HR_LAUNCH_CHECK();
   }
@@ -368,6 +496,10 @@ int hrgpu_force_fermion_core(void *Xs, void *Ys, int auto_fill_odd, double dt, d
 
 int hrgpu_force_clover_logdet(double mass, double residue) {
   HR_REQUIRE(L.ready && L.clover, HRGPU_E_STATE, "force_clover_logdet: no clover term");
+  // the exponential clover blocks are traceless: det D_oo does not depend on the
+  // links and there is no log-det force (the reference has the function for
+  // WITH_CLOVER only, force_fermion_core.c:776-782)
+  if (L.expclover) return 0;
   if (int rc = clover_prepare(mass, HRGPU_DOUBLE)) return rc;
   Geo g = make_geo();
   HR_NF_DISPATCH(L.real, L.nf, (k_force_logdet<N_, R_><<<nb(L.VH), 128, 0, L.stream>>>(L.cl_force, L.cl_idg, L.cl_iod, g, residue)));

@@ -106,39 +106,6 @@ __global__ void k_force0(double *mom, const double2 *Ug, const double2 *gT, Geo 
   for (int A = 0; A < dimg; A++) mom[((long)mu * dimg + A) * lp + d] += coeff * fund_project<N>(b, gT, A);
 }
 
-// e = exp(x), scaling and squaring of the Taylor series (the reference's
-// suNg_Exp is exact to rounding as well)
-template <int N>
-__device__ void mexp(CMat<N> &e, const CMat<N> &x) {
-  double nrm = 0;
-  for (int k = 0; k < N * N; k++) nrm += x.c[k].x * x.c[k].x + x.c[k].y * x.c[k].y;
-  nrm = sqrt(nrm);
-  int sq = 0;
-  while (nrm > 0.25 && sq < 60) {
-    nrm *= 0.5;
-    sq++;
-  }
-  const double scale = ldexp(1.0, -sq);
-  CMat<N> a, term, tmp;
-  for (int k = 0; k < N * N; k++) {
-    a.c[k] = make_double2(x.c[k].x * scale, x.c[k].y * scale);
-    e.c[k] = make_double2((k % (N + 1) == 0) ? 1.0 : 0.0, 0.0);
-    term.c[k] = e.c[k];
-  }
-  for (int j = 1; j <= 20; j++) {
-    mmul<N, false, false>(tmp, term, a);
-    const double inv = 1.0 / j;
-    for (int k = 0; k < N * N; k++) {
-      term.c[k] = make_double2(tmp.c[k].x * inv, tmp.c[k].y * inv);
-      e.c[k] = cadd(e.c[k], term.c[k]);
-    }
-  }
-  for (int q = 0; q < sq; q++) {
-    mmul<N, false, false>(tmp, e, e);
-    e = tmp;
-  }
-}
-
 // U(x,mu) <- exp(dt sum_A mom_A iT_A) U(x,mu)   (ExpX)
 template <int N>
 __global__ void k_update_gauge(double2 *Ug, const double *mom, const double2 *gT, Geo g, int dimg, double dt) {
@@ -156,7 +123,7 @@ __global__ void k_update_gauge(double2 *Ug, const double *mom, const double2 *gT
       X.c[k].y += h * t[k].x;
     }
   }
-  mexp<N>(E, X);
+  mexp_sq<N>(E, X);  // the reference's suNg_Exp is exact to rounding as well
   mload<N, false>(U, Ug, mu, d, lp);
   mmul<N, false, false>(R, E, U);
   for (int k = 0; k < N * N; k++) Ug[((long)mu * N * N + k) * lp + d] = R.c[k];

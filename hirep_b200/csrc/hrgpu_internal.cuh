@@ -68,6 +68,7 @@ struct Lattice {
   bool have_gauge = false, have_gauge_flt = false, have_fund = false;
   // clover
   bool clover = false;
+  bool expclover = false;         // WITH_EXPCLOVER: diagonal (4+m) exp(A/(4+m))
   double csw = 0.0;
   double sigma = 0xF00F;          // mass term (4+m) the inverse was built for
   double2 *cl_term = nullptr;     // A blocks s0..s3 [4][nf*nf][2*ld]

@@ -4,7 +4,10 @@ update_ghmc (LibHR/Update/update_mt.c:148-260) with two monomials: the
 plaquette gauge action (mon_pg.c; force0.c) and an Nf = 2 Wilson pseudofermion
 on the even sites (mon_hmc.c; force_hmc.c, UPDATE_EO branch), integrated with
 the second-order Omelyan integrator (integrators.c:64-93, lambda =
-0.1931833275037836).  Links, momenta and pseudofermions stay on the device; the
+0.1931833275037836).  With the exponential clover term (WITH_EXPCLOVER) the
+fermion operator is Cphi_eopre (D_update.c:26-95) and the monomial has no
+log-det term (the blocks are traceless, det D_oo is constant); the clover
+force is part of force_fermion_core.  Links, momenta and pseudofermions stay on the device; the
 host only holds the scalars of the recursion and the random numbers.
 
 The force solves are either HiRep's (two g5QMR solves on D) or, as the
@@ -24,14 +27,18 @@ LAMBDA_O2MN = 0.1931833275037836
 class HMC:
     def __init__(self, lat, beta, mass, tau, nsteps, force_err2=1e-20, mt_err2=1e-28, force_solver="cg_mixed",
                  bc_t_antiperiodic=True):
-        if lat.csw is not None:
-            # the clover monomial also needs force_clover_logdet and clover_la_logdet
-            raise NotImplementedError("HMC driver: Wilson fermions only (no clover log-det terms)")
+        if lat.csw is not None and not lat.expclover:
+            # the standard clover monomial also needs force_clover_logdet and clover_la_logdet
+            raise NotImplementedError("HMC driver: Wilson or exponential clover fermions (no clover log-det terms)")
         if force_solver not in ("cg_mixed", "cg", "g5qmr"):
             raise ValueError("force_solver: cg_mixed, cg or g5qmr")
         self.lat, self.beta, self.mass, self.tau, self.nsteps = lat, beta, mass, tau, nsteps
         self.force_err2, self.mt_err2, self.force_solver = force_err2, mt_err2, force_solver
         self.bc = bc_t_antiperiodic
+        clover = lat.csw is not None
+        self.op_d = G.OP_CPHI_EOPRE if clover else G.OP_DPHI_EOPRE
+        self.op_h2 = G.OP_G5CPHI_EOPRE_SQ if clover else G.OP_G5DPHI_EOPRE_SQ
+        self.apply_h = lat.g5Cphi_eopre if clover else lat.g5Dphi_eopre
         E = G.EVEN
         self.pf, self.x, self.y, self.tmp = (lat.field(E) for _ in range(4))
         self.Xs, self.Ys = lat.field(G.FULL), lat.field(G.FULL)
@@ -56,18 +63,18 @@ class HMC:
             # X = H^-1 pf = D^-1 g5 pf, Y = H^-1 X = D^-1 g5 X
             lat.la("g5", self.tmp, self.pf)
             lat.la("zero", self.x)
-            it, ok = lat.g5QMR_mshift(G.OP_DPHI_EOPRE, self.mass, [0.0], self.force_err2, self.tmp, [self.x])
+            it, ok = lat.g5QMR_mshift(self.op_d, self.mass, [0.0], self.force_err2, self.tmp, [self.x])
             lat.la("g5", self.tmp, self.x)
             lat.la("zero", self.y)
-            it2, ok2 = lat.g5QMR_mshift(G.OP_DPHI_EOPRE, self.mass, [0.0], self.force_err2, self.tmp, [self.y])
+            it2, ok2 = lat.g5QMR_mshift(self.op_d, self.mass, [0.0], self.force_err2, self.tmp, [self.y])
             self.iters += it + it2
             if not (ok and ok2):
                 raise G.HRGPUError("HMC: g5QMR force solve did not converge")
             X, Y = self.x, self.y
         else:
             # Y = (H^2)^-1 pf (start from the previous solution), X = H Y
-            self._solve(G.OP_G5DPHI_EOPRE_SQ, self.y, self.pf, self.force_err2, self.force_solver == "cg_mixed")
-            lat.g5Dphi_eopre(self.mass, self.x, self.y)
+            self._solve(self.op_h2, self.y, self.pf, self.force_err2, self.force_solver == "cg_mixed")
+            self.apply_h(self.mass, self.x, self.y)
             X, Y = self.x, self.y
         self._even_into_full(self.Xs, X)
         self._even_into_full(self.Ys, Y)
@@ -110,7 +117,7 @@ class HMC:
         eta = lat.field(G.EVEN, host=eta_h)
         lat.local_hmc_action(False, self.beta)
         lat.pf_local_action(eta)
-        lat.g5Dphi_eopre(self.mass, self.pf, eta)  # correct_pf: pf = H eta
+        self.apply_h(self.mass, self.pf, eta)  # correct_pf: pf = H eta
         lat.la("zero", self.y)
         self.iters = 0
         self.nforce = 0
@@ -120,7 +127,7 @@ class HMC:
         # correct_la_pf: pf <- H^-1 pf = D^-1 g5 pf (g5QMR, FP64, MT precision)
         lat.la("g5", self.tmp, self.pf)
         lat.la("zero", self.pf)
-        it, ok = lat.g5QMR_mshift(G.OP_DPHI_EOPRE, self.mass, [0.0], self.mt_err2, self.tmp, [self.pf])
+        it, ok = lat.g5QMR_mshift(self.op_d, self.mass, [0.0], self.mt_err2, self.tmp, [self.pf])
         if not ok:
             raise G.HRGPUError("HMC: accept/reject solve did not converge")
         lat.local_hmc_action(True, self.beta)

@@ -158,6 +158,7 @@ class Lattice:
         self.real = repr_ == ADJ
         self.dimg = ng * ng - 1
         self.csw = None  # clover coefficient once clover_init was called
+        self.expclover = False  # the exponential form (expclover_init)
 
     def nsites(self, par):
         return self.V if par == FULL else self.VH
@@ -228,6 +229,12 @@ class Lattice:
     def clover_init(self, csw):
         _check(self.L.hrgpu_clover_init(D(csw)), "clover_init")
         self.csw = csw
+        self.expclover = False
+
+    def expclover_init(self, csw):
+        _check(self.L.hrgpu_expclover_init(D(csw)), "expclover_init")
+        self.csw = csw
+        self.expclover = True
 
     def compute_clover_term(self):
         _check(self.L.hrgpu_compute_clover_term(), "compute_clover_term")

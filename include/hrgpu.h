@@ -168,6 +168,12 @@ int hrgpu_D(void *out, const void *in);
 
 /* ---------------------------------------------------------------- clover -- */
 int hrgpu_clover_init(double csw);                  /* clover_init, clover_tools.c:360-373        */
+/* the same with the exponential clover term of WITH_EXPCLOVER (Dphi.c:1292-1482,
+ * LibHR/Utils/clover_exp.c): diagonal (4+m) exp(A/(4+m)), inverse
+ * exp(-A/(4+m))/(4+m); every Cphi operator and force_fermion_core then use it
+ * (force_fermion_core.c:484-772), and force_clover_logdet adds nothing (the
+ * blocks are traceless: det D_oo is constant). */
+int hrgpu_expclover_init(double csw);
 int hrgpu_compute_clover_term(void);                /* compute_clover_term, clover_tools.c:333-341 */
 int hrgpu_compute_ldl_decomp(double sigma);         /* compute_ldl_decomp, clover_tools.c:343-358  */
 int hrgpu_clover_term_get(void *cl_host);           /* cl_term in HiRep layout [V][4][NF*NF] complex */
@@ -350,7 +356,7 @@ int hrgpu_fermion_force_begin(void);                    /* force_fermion_core.c:
  * full-lattice device fields; with auto_fill_odd their odd halves are overwritten
  * by D_oe (times D_oo^-1 with clover) of the even halves, as in the reference. */
 int hrgpu_force_fermion_core(void *Xs, void *Ys, int auto_fill_odd, double dt, double residue);
-int hrgpu_force_clover_logdet(double mass, double residue); /* force_fermion_core.c:777-781 */
+int hrgpu_force_clover_logdet(double mass, double residue); /* force_fermion_core.c:777-781; no-op for expclover */
 /* fermion_force_end (force_fermion_core.c:964-993): clover derivative, then adds the
  * accumulated force to the host momentum field force[V][4][NG*NG-1] (HiRep layout) */
 int hrgpu_fermion_force_end(double dt, double *force_host);

@@ -926,14 +926,92 @@ void orc_g5Dphi_eopre_sq_flt(double m0, fcplx *out, const fcplx *in)
 #define LDLN (NF_ * (2 * NF_ + 1)) /* packed lower-triangular 2NF x 2NF        */
 #define CPX(x, i, j) ((x)[(i) * ((i) + 1) / 2 + (j)])
 
+static int expclover_ = 0; /* WITH_EXPCLOVER: diagonal (4+m) exp(A/(4+m)) */
+
 void orc_clover_init(double csw)
 {
+  expclover_ = 0;
   free(cl_term_); free(cl_ldl_); free(cl_force_);
   cl_term_ = calloc((size_t)V_ * 4 * NF_ * NF_, sizeof(cplx));
   cl_ldl_ = calloc((size_t)V_ * 2 * LDLN, sizeof(cplx));
   cl_force_ = calloc((size_t)V_ * 6 * NF_ * NF_, sizeof(cplx));
   csw_ = csw;
   sigma_ = 0xF00F;
+}
+
+/* exponential clover (Dphi.c:1292-1482, LibHR/Utils/clover_exp.c): the same
+ * clover term, the diagonal (4+m) exp(A/(4+m)) and its inverse exp(-A/(4+m))/(4+m) */
+void orc_expclover_init(double csw)
+{
+  orc_clover_init(csw);
+  expclover_ = 1;
+}
+
+/* block b (0: [[s0, s1], [s1^+, -s0]], 1: the same from s2, s3) of site ix, dense 2NF x 2NF */
+static void clover_block(cplx *m, int ix, int b)
+{
+  const int F = NF_, F2 = NF_ * NF_, n = 2 * NF_;
+  const cplx *sa = cl_term_ + ((size_t)ix * 4 + 2 * b) * F2, *sb = sa + F2;
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++)
+    {
+      cplx v;
+      if (i < F && j < F) v = sa[i * F + j];
+      else if (i < F) v = sb[i * F + (j - F)];
+      else if (j < F) v = conj(sb[j * F + (i - F)]);
+      else v = -sa[(i - F) * F + (j - F)];
+      m[i * n + j] = v;
+    }
+}
+
+/* exp(x) of an n x n matrix by its Taylor series, summed until the terms' norm
+ * is below 1e-28 (clover_exp_taylor, clover_exp.c:364-396) */
+static void taylor_exp(int n, cplx *e, const cplx *x)
+{
+  cplx term[n * n], tmp[n * n];
+  for (int k = 0; k < n * n; k++) e[k] = term[k] = (k % (n + 1) == 0) ? 1.0 : 0.0;
+  for (int j = 1; j < 200; j++)
+  {
+    mat_mul(n, tmp, term, x);
+    double nrm = 0;
+    for (int k = 0; k < n * n; k++)
+    {
+      term[k] = tmp[k] / j;
+      e[k] += term[k];
+      nrm += creal(term[k] * conj(term[k]));
+    }
+    if (sqrt(nrm) < 1e-28) break;
+  }
+}
+
+/* out = (4+m)^s exp(s A/(4+m)) in on the chiral halves, s = +1 (Cphi_) or -1 (inverse) */
+static void expclover_apply(double mass, cplx *out, const cplx *in, int par, int assign, int inverse)
+{
+  const int F = NF_, n = 2 * NF_;
+  const double sig = 4. + mass, c = (inverse ? -1.0 : 1.0) / sig, scale = inverse ? 1.0 / sig : sig;
+  const int b0 = par_base(par);
+#pragma omp parallel for
+  for (int ix = b0; ix < par_end(par); ix++)
+  {
+    const cplx *s = in + (size_t)(ix - b0) * SPN;
+    cplx tmp[4 * 64];
+    for (int b = 0; b < 2; b++)
+    {
+      cplx m[n * n], e[n * n];
+      clover_block(m, ix, b);
+      for (int k = 0; k < n * n; k++) m[k] *= c;
+      taylor_exp(n, e, m);
+      for (int i = 0; i < n; i++)
+      {
+        cplx v = 0;
+        for (int j = 0; j < n; j++) v += e[i * n + j] * s[2 * b * F + j];
+        tmp[2 * b * F + i] = scale * v;
+      }
+    }
+    cplx *o = out + (size_t)(ix - b0) * SPN;
+    for (int k = 0; k < SPN; k++)
+      if (assign) o[k] += tmp[k]; else o[k] = tmp[k];
+  }
 }
 
 /* a generic represented link as complex (real reps promoted) */
@@ -1117,6 +1195,11 @@ void orc_compute_ldl_decomp(double sigma0)
 /* Dphi.c:1091-1146 */
 void orc_Cphi_(double mass, cplx *out, const cplx *in, int par, int assign)
 {
+  if (expclover_)
+  {
+    expclover_apply(mass, out, in, par, assign, 0);
+    return;
+  }
   int F = NF_, F2 = NF_ * NF_;
   mass = 4. + mass;
   int b = par_base(par);
@@ -1154,6 +1237,11 @@ void orc_Cphi_(double mass, cplx *out, const cplx *in, int par, int assign)
 /* Dphi.c:1148-1213 (LDL forward/back substitution) */
 void orc_Cphi_inv_(double mass, cplx *out, const cplx *in, int par, int assign)
 {
+  if (expclover_)
+  {
+    expclover_apply(mass, out, in, par, assign, 1);
+    return;
+  }
   int N = 2 * NF_;
   mass = 4. + mass;
   orc_compute_ldl_decomp(mass);
@@ -1940,6 +2028,87 @@ static void force_clover_fermion(const cplx *Xs, const cplx *Ys, double residue)
   }
 }
 
+/* the truncation order of the exponential clover's Taylor forms, from csw and
+ * the mass as evaluate_sw_order chooses it (clover_exp.c:70-100): the smallest n
+ * with c^(n+1) e^c < eps (n+1)!, c = 3 csw/(4+m); the series then runs to n+2 */
+static int sw_exp_order(double mass)
+{
+  const double c = 3.0 * csw_ / (4.0 + mass);
+  double a = c * exp(c), b = 2.220446049250313e-16;
+  for (int n = 1; n < 100; n++)
+  {
+    a *= c;
+    b *= (double)(n + 1);
+    if (a < b) return n + 2;
+  }
+  return 101; /* the reference stops here with "SW parameters are out of range" */
+}
+
+/* the exponential clover's force matrices (force_clover_fermion_taylor,
+ * force_fermion_core.c:631-772): with A the clover block over 4+m,
+ * rhs_k = A^k X, xi_l = A^l Y, lhs_k = sum_l C_kl xi_l, C_kl = 1/(k+l+1)! for
+ * k+l <= n (factorialCoef, clover_exp.c:566-592), and the same sigma insertions
+ * as the linear term for every k.  The reference takes the Cayley-Hamilton
+ * coefficients (doublehorner, clover_exp.c:398-563) for NF = 2, 3: the same
+ * derivative of the exponential, to rounding. */
+static void force_expclover_fermion(const cplx *Xs, const cplx *Ys, double residue)
+{
+  const int F = NF_, n2 = 2 * NF_, F2 = NF_ * NF_;
+  const int nexp = sw_exp_order(static_mass_);
+  const double inv = 1.0 / (4.0 + static_mass_);
+  static const int mn[6][2] = {{0, 1}, {0, 2}, {1, 2}, {0, 3}, {1, 3}, {2, 3}};
+  double *fact = malloc(sizeof(double) * (2 * nexp + 2));
+  fact[0] = 1.0;
+  for (int k = 1; k < 2 * nexp + 2; k++) fact[k] = fact[k - 1] / k;
+#pragma omp parallel for
+  for (int ix = 0; ix < V_; ix++)
+  {
+    cplx a[2][n2 * n2];
+    cplx *xi = malloc(sizeof(cplx) * (size_t)nexp * SPN);
+    cplx rhs[4 * 64], lhs[4 * 64], tl[4 * 64], tr[4 * 64], fm[F2];
+    for (int b = 0; b < 2; b++)
+    {
+      clover_block(a[b], ix, b);
+      for (int k = 0; k < n2 * n2; k++) a[b][k] *= inv;
+    }
+    /* spinor <- A spinor, block by block */
+#define APPLY_A(out, in)                                                          \
+  for (int b = 0; b < 2; b++)                                                     \
+    for (int i = 0; i < n2; i++)                                                  \
+    {                                                                             \
+      cplx v = 0;                                                                 \
+      for (int j = 0; j < n2; j++) v += a[b][i * n2 + j] * (in)[2 * b * F + j];   \
+      (out)[2 * b * F + i] = v;                                                   \
+    }
+    memcpy(xi, Ys + (size_t)ix * SPN, sizeof(cplx) * SPN);
+    for (int k = 0; k + 1 < nexp; k++) { APPLY_A(xi + (size_t)(k + 1) * SPN, xi + (size_t)k * SPN) }
+    memcpy(rhs, Xs + (size_t)ix * SPN, sizeof(cplx) * SPN);
+    for (int k = 0; k < nexp; k++)
+    {
+      if (k > 0)
+      {
+        cplx t[4 * 64];
+        APPLY_A(t, rhs)
+        memcpy(rhs, t, sizeof(cplx) * SPN);
+      }
+      for (int c = 0; c < SPN; c++) lhs[c] = 0;
+      for (int l = 0; l < nexp && k + l <= nexp; l++)
+        for (int c = 0; c < SPN; c++) lhs[c] += fact[k + l + 1] * xi[(size_t)l * SPN + c];
+      for (int q = 0; q < 6; q++)
+      {
+        g5_sigma(tr, rhs, mn[q][0], mn[q][1]);
+        g5_sigma(tl, lhs, mn[q][0], mn[q][1]);
+        fmat_create(fm, tl, rhs, tr, lhs);
+        cplx *cf = cl_force_ + ((size_t)ix * 6 + q) * F2;
+        for (int e = 0; e < F2; e++) cf[e] += residue * fm[e];
+      }
+    }
+#undef APPLY_A
+    free(xi);
+  }
+  free(fact);
+}
+
 static void av_mul_add(double *f, double c, const double *h)
 {
   for (int A = 0; A < DIMG_; A++) f[A] += c * h[A];
@@ -2026,7 +2195,11 @@ void orc_force_fermion_core(cplx *Xs, cplx *Ys, int auto_fill_odd, double dt, do
     }
   }
   coeff = -coeff;
-  if (cl_term_) force_clover_fermion(Xs, Ys, residue);
+  if (cl_term_)
+  {
+    if (expclover_) force_expclover_fermion(Xs, Ys, residue);
+    else force_clover_fermion(Xs, Ys, residue);
+  }
 #pragma omp parallel for
   for (int ix = 0; ix < V_; ix++)
   {
@@ -2053,6 +2226,10 @@ void orc_force_fermion_core(cplx *Xs, cplx *Ys, int auto_fill_odd, double dt, do
 /* _compute_clover_force + compute_force_logdet (clover_tools.c:208-310) */
 void orc_force_clover_logdet(double mass, double coeff)
 {
+  /* the exponential clover blocks are traceless, det D_oo does not depend on
+   * the links: no log-det force (force_clover_logdet exists for WITH_CLOVER only,
+   * force_fermion_core.c:776-782) */
+  if (expclover_) return;
   int F = NF_, N2 = 2 * NF_, F2 = NF_ * NF_;
   orc_compute_ldl_decomp(4.0 + mass);
 #pragma omp parallel for

@@ -72,6 +72,7 @@ void orc_g5Dphi_eopre_flt(double m0, float complex *out, const float complex *in
 void orc_g5Dphi_eopre_sq_flt(double m0, float complex *out, const float complex *in);
 
 /* clover (LibHR/Update/clover_tools.c, Dphi.c:1081-1290) */
+void orc_expclover_init(double csw);
 void orc_clover_init(double csw);
 void orc_compute_clover_term(void);
 void orc_compute_ldl_decomp(double sigma0);

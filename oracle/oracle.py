@@ -178,6 +178,10 @@ class Oracle:
     def clover_init(self, csw):
         self.L.orc_clover_init(ctypes.c_double(csw))
 
+    def expclover_init(self, csw):
+        """WITH_EXPCLOVER: diagonal (4+m) exp(A/(4+m)) (Dphi.c:1292-1482)."""
+        self.L.orc_expclover_init(ctypes.c_double(csw))
+
     def compute_clover_term(self):
         self.L.orc_compute_clover_term()
 

@@ -1,0 +1,73 @@
+"""An HMC trajectory driven entirely by the oracle: update_ghmc
+(LibHR/Update/update_mt.c:148-260) with the plaquette monomial and an Nf=2
+Wilson or exponential clover pseudofermion on the even sites, O2MN integration
+(integrators.c:64-93).  Test infrastructure: the GPU driver's trajectories are
+checked against it, and its own dH ~ dt^2 pins the oracle's forces."""
+import numpy as np
+
+import oracle as O
+
+
+def oracle_trajectory(o, u0, beta, mass, tau, nsteps, rng, force_err2, mt_err2, expclover_csw=None):
+    """update_ghmc with the plaquette and Nf=2 Wilson (or exponential clover)
+    monomials and O2MN, every piece from the oracle (the same random numbers as
+    hirep_b200.hmc.HMC.trajectory)."""
+    lam = 0.1931833275037836
+    V, VH, nf, dimg = o.V, o.VH, o.nf, o.dimg
+    g5 = np.array([1, 1, -1, -1])[None, :, None]
+    keep = {}
+    clover = expclover_csw is not None
+    if clover:
+        o.expclover_init(expclover_csw)
+    op_h2 = O.OP_G5CPHI_EOPRE_SQ if clover else O.OP_G5DPHI_EOPRE_SQ
+    op_d = O.OP_CPHI_EOPRE if clover else O.OP_DPHI_EOPRE
+    apply_h = o.g5Cphi_eopre if clover else o.g5Dphi_eopre
+
+    def represent(u):
+        keep["uf"] = o.represent_gauge_field(u, True)
+        o.set_gauge(keep["uf"])
+        if clover:
+            o.compute_clover_term()
+
+    u = u0.copy()
+    represent(u)
+    o.set_mass(mass)
+    mom = rng.standard_normal((V, 4, dimg)) / np.sqrt(0.5)
+    eta = (rng.standard_normal((VH, 4, nf)) + 1j * rng.standard_normal((VH, 4, nf))) / np.sqrt(2)
+    H0 = o.local_hmc_action(beta, u, mom).sum() + np.sum(np.abs(eta) ** 2)
+    pf = apply_h(mass, eta)
+    st = {"y": np.zeros_like(eta), "count": 0, "u": u, "mom": mom}
+
+    def force(dt):
+        st["mom"] = o.force0(dt, beta, st["u"], st["mom"])
+        y, _ = o.cg_mshift(op_h2, [0.0], force_err2, pf, guess=st["y"])
+        st["y"] = y[0]
+        x = apply_h(mass, st["y"])
+        Xs = np.zeros((V, 4, nf), complex)
+        Ys = np.zeros_like(Xs)
+        Xs[:VH], Ys[:VH] = x, st["y"]
+        o.fermion_force_begin()
+        o.force_fermion_core(Xs, Ys, 1, dt, 1.0)
+        st["mom"] = o.fermion_force_end(dt, st["mom"])
+
+    def field(dt):
+        st["u"] = o.update_gauge_field(dt, st["u"], st["mom"])
+        if st["count"] & 16:  # field_update.c:45-57
+            st["count"] = 0
+            st["u"] = o.project_gauge_field(st["u"])
+        else:
+            st["count"] += 1
+        represent(st["u"])
+
+    dt = tau / nsteps
+    for n in range(nsteps):
+        force(lam * dt if n == 0 else 2 * lam * dt)
+        field(dt / 2)
+        force((1 - 2 * lam) * dt)
+        field(dt / 2)
+    force(lam * dt)
+    st["u"] = o.project_gauge_field(st["u"])
+    represent(st["u"])
+    xo, _ = o.g5QMR_mshift(op_d, [0.0], mt_err2, g5 * pf)
+    H1 = o.local_hmc_action(beta, st["u"], st["mom"]).sum() + np.sum(np.abs(xo[0]) ** 2)
+    return H1 - H0, st["u"]

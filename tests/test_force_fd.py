@@ -30,12 +30,15 @@ def perturbed(u, gT, w, eps):
 
 
 @pytest.mark.parametrize("ng,rep,clover", [(2, O.FUND, False), (2, O.ADJ, False), (3, O.FUND, True),
-                                            (3, O.SYM, False), (4, O.ASYM, False)])
+                                            (3, O.SYM, False), (4, O.ASYM, False), (3, O.FUND, "exp"),
+                                            (2, O.ADJ, "exp")])
 def test_oracle_force_is_minus_twice_action_derivative(ng, rep, clover):
     o = O.Oracle(4, 4, 4, 4, ng, rep)
     m = -0.1
     o.set_mass(m)
-    if clover:
+    if clover == "exp":
+        o.expclover_init(1.0)
+    elif clover:
         o.clover_init(1.0)
     u = F.smooth_gauge(5, o.V, ng, 0.3)
     phi = F.gaussian_spinor(3, o.VH, o.nf)

@@ -9,6 +9,7 @@ import pytest
 import oracle as O
 from hirep_b200 import fields as F
 from hirep_b200 import hrgpu as G
+from hmc_oracle import oracle_trajectory as _oracle_trajectory
 
 pytestmark = pytest.mark.gpu
 
@@ -93,62 +94,6 @@ def test_fermion_force_into_device_momenta():
     assert np.abs(lat.momenta_get() - host).max() < 1e-14
 
 
-def _oracle_trajectory(o, u0, beta, mass, tau, nsteps, rng, force_err2, mt_err2):
-    """update_ghmc with the plaquette and Nf=2 Wilson monomials and O2MN, every piece
-    from the oracle (the same random numbers as hirep_b200.hmc.HMC.trajectory)."""
-    lam = 0.1931833275037836
-    V, VH, nf, dimg = o.V, o.VH, o.nf, o.dimg
-    g5 = np.array([1, 1, -1, -1])[None, :, None]
-    keep = {}
-
-    def represent(u):
-        keep["uf"] = o.represent_gauge_field(u, True)
-        o.set_gauge(keep["uf"])
-
-    u = u0.copy()
-    represent(u)
-    o.set_mass(mass)
-    mom = rng.standard_normal((V, 4, dimg)) / np.sqrt(0.5)
-    eta = (rng.standard_normal((VH, 4, nf)) + 1j * rng.standard_normal((VH, 4, nf))) / np.sqrt(2)
-    H0 = o.local_hmc_action(beta, u, mom).sum() + np.sum(np.abs(eta) ** 2)
-    pf = o.g5Dphi_eopre(mass, eta)
-    st = {"y": np.zeros_like(eta), "count": 0, "u": u, "mom": mom}
-
-    def force(dt):
-        st["mom"] = o.force0(dt, beta, st["u"], st["mom"])
-        y, _ = o.cg_mshift(O.OP_G5DPHI_EOPRE_SQ, [0.0], force_err2, pf, guess=st["y"])
-        st["y"] = y[0]
-        x = o.g5Dphi_eopre(mass, st["y"])
-        Xs = np.zeros((V, 4, nf), complex)
-        Ys = np.zeros_like(Xs)
-        Xs[:VH], Ys[:VH] = x, st["y"]
-        o.fermion_force_begin()
-        o.force_fermion_core(Xs, Ys, 1, dt, 1.0)
-        st["mom"] = o.fermion_force_end(dt, st["mom"])
-
-    def field(dt):
-        st["u"] = o.update_gauge_field(dt, st["u"], st["mom"])
-        if st["count"] & 16:  # field_update.c:45-57
-            st["count"] = 0
-            st["u"] = o.project_gauge_field(st["u"])
-        else:
-            st["count"] += 1
-        represent(st["u"])
-
-    dt = tau / nsteps
-    for n in range(nsteps):
-        force(lam * dt if n == 0 else 2 * lam * dt)
-        field(dt / 2)
-        force((1 - 2 * lam) * dt)
-        field(dt / 2)
-    force(lam * dt)
-    st["u"] = o.project_gauge_field(st["u"])
-    represent(st["u"])
-    xo, _ = o.g5QMR_mshift(O.OP_DPHI_EOPRE, [0.0], mt_err2, g5 * pf)
-    H1 = o.local_hmc_action(beta, st["u"], st["mom"]).sum() + np.sum(np.abs(xo[0]) ** 2)
-    return H1 - H0, st["u"]
-
-
 def test_hmc_trajectory_matches_oracle_trajectory():
     """One O2MN trajectory (10 steps, 20 link updates: one reunitarisation) of the
     SU(2) adjoint Nf=2 Wilson + plaquette system: dH and the final links."""
@@ -166,6 +111,27 @@ def test_hmc_trajectory_matches_oracle_trajectory():
     assert abs(res["dH"] - dH_o) < 1e-8 * max(1.0, abs(dH_o)), (res["dH"], dH_o)
     assert np.abs(lat.gauge_get() - u_o).max() < 1e-10
     assert res["force_evaluations"] == 2 * 10 + 1  # O2MN: two per step and a last one
+
+
+def test_hmc_expclover_trajectory_matches_oracle_trajectory():
+    """The same with Nf=2 exponential clover fermions (WITH_EXPCLOVER, csw=1.2),
+    SU(3) fundamental: the clover term rebuilt after every link update, the
+    force with the exponential's derivative, no log-det term."""
+    from hirep_b200.hmc import HMC
+
+    dims, ng, beta, mass, csw = (4, 4, 4, 4), 3, 5.6, -0.3, 1.2
+    o = O.Oracle(*dims, ng, O.FUND)
+    u0 = F.smooth_gauge(98, o.V, ng, 0.2)
+    lat = G.Lattice(*dims, ng, G.FUND, ipt=o.geometry()[0])
+    lat.set_gauge(u0)
+    lat.represent_gauge_field(True)
+    lat.expclover_init(csw)
+    hmc = HMC(lat, beta, mass, tau=0.5, nsteps=8, force_err2=1e-26, mt_err2=1e-28, force_solver="cg")
+    res = hmc.trajectory(np.random.default_rng(15), metropolis=False)
+    dH_o, u_o = _oracle_trajectory(o, u0, beta, mass, 0.5, 8, np.random.default_rng(15), 1e-26, 1e-28,
+                                   expclover_csw=csw)
+    assert abs(res["dH"] - dH_o) < 1e-8 * max(1.0, abs(dH_o)), (res["dH"], dH_o)
+    assert np.abs(lat.gauge_get() - u_o).max() < 1e-10
 
 
 @pytest.mark.parametrize("solver", ["cg_mixed", "g5qmr"])

@@ -385,3 +385,69 @@ def test_pure_gauge_leapfrog_energy_violation_scales_as_dt_squared():
 
     d1, d2 = dH(10), dH(20)
     assert 3.5 < d1 / d2 < 4.5, (d1, d2)  # leapfrog: dH = O(dt^2)
+
+
+# ---- exponential clover (Dphi.c:1292-1482, LibHR/Utils/clover_exp.c)
+def _expclover_oracle(csw=1.0, ng=3, rep=O.FUND):
+    o = O.Oracle(4, 4, 4, 4, ng, rep)
+    o.set_gauge(o.represent_gauge_field(F.smooth_gauge(5, o.V, ng, 0.4), True))
+    o.expclover_init(csw)
+    o.compute_clover_term()
+    return o
+
+
+def test_expclover_diag_times_inverse_is_identity_and_matches_expm():
+    import scipy.linalg as sl
+
+    o = _expclover_oracle()
+    m = -0.2
+    e = F.gaussian_spinor(1, o.VH, o.nf)
+    back = o.Cphi_diag_inv(m, o.Cphi_diag(m, e, O.EVEN), O.EVEN)
+    assert np.abs(back - e).max() < 1e-13
+    # site 0, chiral block 0 against scipy's expm of [[s0, s1], [s1^+, -s0]] / (4+m)
+    cl = o.clover_term()[0]
+    nf = o.nf
+    A = np.block([[cl[0], cl[1]], [cl[1].conj().T, -cl[0]]])
+    E = (4 + m) * sl.expm(A / (4 + m))
+    v = np.zeros((o.VH, 4, nf), complex)
+    v[0, 0, 0] = 1.0
+    col = o.Cphi_diag(m, v, O.EVEN)[0, :2].reshape(-1)
+    assert np.abs(col - E[:, 0]).max() < 1e-13
+
+
+def test_expclover_is_the_clover_operator_at_small_csw():
+    m = -0.2
+    e = F.gaussian_spinor(2, 128, 3)
+    out = {}
+    for exp_, csw in ((True, 1e-4), (False, 1e-4)):
+        o = O.Oracle(4, 4, 4, 4, 3, O.FUND)
+        o.set_gauge(o.represent_gauge_field(F.smooth_gauge(5, o.V, 3, 0.4), True))
+        (o.expclover_init if exp_ else o.clover_init)(csw)
+        o.compute_clover_term()
+        out[exp_] = o.Cphi_eopre(m, e)
+    assert 0 < np.abs(out[True] - out[False]).max() / np.abs(out[False]).max() < 1e-8
+
+
+def test_expclover_eopre_sq_hermitian():
+    o = _expclover_oracle()
+    m = -0.2
+    a, b = F.gaussian_spinor(3, o.VH, o.nf), F.gaussian_spinor(4, o.VH, o.nf)
+    lhs = np.vdot(a, o.g5Cphi_eopre_sq(m, b))
+    rhs = np.vdot(o.g5Cphi_eopre_sq(m, a), b)
+    assert abs(lhs - rhs) < 1e-12 * abs(lhs)
+
+
+def test_expclover_hmc_energy_violation_scales_as_dt_squared():
+    """An oracle HMC trajectory with Nf=2 exponential clover fermions (csw=1.2,
+    SU(3) fundamental, 4^4): dH falls as dt^2 (8 -> 16 steps: 3.95), so the
+    exponential clover force is the derivative of the exponential clover action."""
+    from hmc_oracle import oracle_trajectory
+    from hirep_b200 import fields as F
+
+    dh = {}
+    for n in (8, 16):
+        o = O.Oracle(4, 4, 4, 4, 3, O.FUND)
+        u0 = F.smooth_gauge(98, o.V, 3, 0.2)
+        dh[n], _ = oracle_trajectory(o, u0, 5.6, -0.3, 0.5, n, np.random.default_rng(15), 1e-26, 1e-28,
+                                     expclover_csw=1.2)
+    assert 3.5 < dh[8] / dh[16] < 4.5, dh
