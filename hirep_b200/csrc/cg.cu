@@ -230,6 +230,7 @@ void cg_release() {
   batch_release();
   qmr_release();
   hmc_release();
+  hostop_release();
   cudaFree(FW.dres); cudaFree(FW.dres2); cudaFree(FW.dtmp);
   for (void *b : FW.fbuf) cudaFree(b);
   FW = FltWork();

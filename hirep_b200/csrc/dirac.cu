@@ -28,8 +28,11 @@ static const void *links() {
 // one hop onto parity outp with the given epilogue; fields are parity fields
 template <typename R>
 int hop(int outp, void *out, const void *in, int ep, double cacc, const void *aux, double caux, int g5, double *red,
-        const R *cdg, const typename C2<R>::T *cod) {
+        const R *cdg, const typename C2<R>::T *cod, int cb0, int cb1) {
   HopArgs<R> a;
+  a.cb0 = cb0;
+  a.cb1 = cb1 < 0 ? (int)L.VH : cb1;
+  if (a.cb1 <= a.cb0) return 0;
   a.in = in;
   a.out = out;
   a.U = links<R>();
@@ -46,13 +49,13 @@ int hop(int outp, void *out, const void *in, int ep, double cacc, const void *au
     if (int rc = ensure_links_bf16()) return rc;
     a.U = L.Ubf;
   }
-  g_mvm++;
+  if (a.cb0 == 0 && a.cb1 == (int)L.VH) g_mvm++;  // partial launches are counted by their caller
   return launch_hop<R>(ep, a);
 }
 template int hop<double>(int, void *, const void *, int, double, const void *, double, int, double *, const double *,
-                         const double2 *);
+                         const double2 *, int, int);
 template int hop<float>(int, void *, const void *, int, double, const void *, double, int, double *, const float *,
-                        const float2 *);
+                        const float2 *, int, int);
 
 int check_gauge(int prec) {
   HR_REQUIRE(L.ready, HRGPU_E_STATE, "lattice not initialised");
@@ -104,22 +107,45 @@ int Dphi_full(double m0, void *out, const void *in, int g5) {
   return 0;
 }
 
+// one hop of an even-odd preconditioned operator with output parity p, on the
+// output sites cb0 <= cb < cb1 of its parity:
+//   stage 0: tmp = D_qp in on parity q = 1-p (clover: times D_qq^-1)
+//   stage 1: out = rho in + 1/2 D_pq tmp with rho = (4+m)^2 (Wilson), or
+//            D_pp in + 1/2 D_pq tmp (clover), optionally times gamma_5.
+// Stage 1 on a range needs stage 0 done on the neighbouring range (one site
+// further in every direction).
+template <typename R>
+int eo_stage(int clover, double mass, int stage, int outp, void *out, const void *in, int g5, double *red, int cb0,
+             int cb1) {
+  void **tmp = sizeof(R) == 8 ? &L.tmp_o : &L.tmp_o_f;
+  if (int rc = ensure_tmp(tmp, spinor_bytes(HRGPU_EVEN, sizeof(R) == 8 ? HRGPU_DOUBLE : HRGPU_FLOAT))) return rc;
+  if (clover) {
+    const R *idg, *ddg;
+    const typename C2<R>::T *iod, *dod;
+    clover_blocks<R>(&ddg, &dod, &idg, &iod);
+    if (stage == 0) return hop<R>(outp ^ 1, *tmp, in, EP_CLOV_INV, -0.5, nullptr, 0.0, 0, nullptr, idg, iod, cb0, cb1);
+    return hop<R>(outp, out, *tmp, EP_CLOV, 0.5, in, 0.0, g5, red, ddg, dod, cb0, cb1);
+  }
+  if (stage == 0) return hop<R>(outp ^ 1, *tmp, in, EP_AXPY, -0.5, nullptr, 0.0, 0, nullptr, nullptr, nullptr, cb0, cb1);
+  double rho = 4.0 + mass;
+  if (sizeof(R) == 4) {
+    float r = 4.f + (float)mass;
+    rho = (double)(r * r);
+  } else {
+    rho = rho * rho;
+  }
+  return hop<R>(outp, out, *tmp, EP_AXPY, 0.5, in, rho, g5, red, nullptr, nullptr, cb0, cb1);
+}
+template int eo_stage<double>(int, double, int, int, void *, const void *, int, double *, int, int);
+template int eo_stage<float>(int, double, int, int, void *, const void *, int, double *, int, int);
+
 // even-odd: out = (4+m)^2 in - D_pq D_qp in on parity p, optionally gamma_5
 template <typename R>
 int Dphi_eo(double m0, void *out, const void *in, int outp, int g5, double *red) {
   if (int rc = check_gauge(sizeof(R) == 8 ? HRGPU_DOUBLE : HRGPU_FLOAT)) return rc;
   HR_REQUIRE(out && in && out != in, HRGPU_E_ARG, "Dphi_eopre: input and output fields must be different");
-  void **tmp = sizeof(R) == 8 ? &L.tmp_o : &L.tmp_o_f;
-  if (int rc = ensure_tmp(tmp, spinor_bytes(HRGPU_EVEN, sizeof(R) == 8 ? HRGPU_DOUBLE : HRGPU_FLOAT))) return rc;
-  if (int rc = hop<R>(outp ^ 1, *tmp, in, EP_AXPY, -0.5, nullptr, 0.0, 0, nullptr, nullptr, nullptr)) return rc;
-  double rho = 4.0 + m0;
-  if (sizeof(R) == 4) {
-    float r = 4.f + (float)m0;
-    rho = (double)(r * r);
-  } else {
-    rho = rho * rho;
-  }
-  return hop<R>(outp, out, *tmp, EP_AXPY, 0.5, in, rho, g5, red, nullptr, nullptr);
+  if (int rc = eo_stage<R>(0, m0, 0, outp, out, in, g5, nullptr, 0, -1)) return rc;
+  return eo_stage<R>(0, m0, 1, outp, out, in, g5, red, 0, -1);
 }
 
 template int Dphi_eo<double>(double, void *, const void *, int, int, double *);
@@ -132,15 +158,8 @@ int Cphi_eo(double mass, void *out, const void *in, int g5, double *red) {
   HR_REQUIRE(L.clover, HRGPU_E_STATE, "Cphi_eopre: no clover term (hrgpu_clover_init)");
   HR_REQUIRE(out && in && out != in, HRGPU_E_ARG, "Cphi_eopre: input and output fields must be different");
   if (int rc = clover_prepare(mass, sizeof(R) == 8 ? HRGPU_DOUBLE : HRGPU_FLOAT)) return rc;
-  void **tmp = sizeof(R) == 8 ? &L.tmp_o : &L.tmp_o_f;
-  if (int rc = ensure_tmp(tmp, spinor_bytes(HRGPU_EVEN, sizeof(R) == 8 ? HRGPU_DOUBLE : HRGPU_FLOAT))) return rc;
-  const R *idg;
-  const typename C2<R>::T *iod;
-  const R *ddg;
-  const typename C2<R>::T *dod;
-  clover_blocks<R>(&ddg, &dod, &idg, &iod);
-  if (int rc = hop<R>(HRGPU_ODD, *tmp, in, EP_CLOV_INV, -0.5, nullptr, 0.0, 0, nullptr, idg, iod)) return rc;
-  return hop<R>(HRGPU_EVEN, out, *tmp, EP_CLOV, 0.5, in, 0.0, g5, red, ddg, dod);
+  if (int rc = eo_stage<R>(1, mass, 0, HRGPU_EVEN, out, in, g5, nullptr, 0, -1)) return rc;
+  return eo_stage<R>(1, mass, 1, HRGPU_EVEN, out, in, g5, red, 0, -1);
 }
 template int Cphi_eo<double>(double, void *, const void *, int, double *);
 template int Cphi_eo<float>(double, void *, const void *, int, double *);

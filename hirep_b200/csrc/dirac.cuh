@@ -10,9 +10,12 @@ int launch_hop(int ep, HopArgs<R> &a);
 
 template <typename R>
 int hop(int outp, void *out, const void *in, int ep, double cacc, const void *aux, double caux, int g5, double *red,
-        const R *cdg, const typename C2<R>::T *cod);
+        const R *cdg, const typename C2<R>::T *cod, int cb0 = 0, int cb1 = -1);
 
 int check_gauge(int prec);
+template <typename R>
+int eo_stage(int clover, double mass, int stage, int outp, void *out, const void *in, int g5, double *red, int cb0,
+             int cb1);
 template <typename R>
 int Dphi_eo(double m0, void *out, const void *in, int outp, int g5, double *red);
 template <typename R>

@@ -39,6 +39,7 @@ struct HopArgs {
   int outp;
   int g5;
   int nf;
+  int cb0, cb1;      // output sites cb0 <= cb < cb1 of parity outp
   Geo g;
 };
 
@@ -351,9 +352,9 @@ __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb) {
 template <int NFT, bool REAL, typename R, int EP, int MINB, typename LE = typename LinkE<REAL, R>::T>
 __global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop(HopArgs<R> a) {
   if (a.stop && *a.stop) return;
-  const int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  const int cb = a.cb0 + blockIdx.x * blockDim.x + threadIdx.x;
   double nrm = 0.0;
-  if (cb < a.g.VH) nrm = hop_site<NFT, REAL, R, EP, LE>(a, cb);
+  if (cb < a.cb1) nrm = hop_site<NFT, REAL, R, EP, LE>(a, cb);
   if (a.red) block_partial<R>(nrm, a.red);
 }
 
@@ -518,8 +519,8 @@ template <int NFT, bool REAL, typename R, int EP, int MINB, typename LE = typena
 __global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop2(HopArgs<R> a) {
   if (a.stop && *a.stop) return;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool active = (tid >> 1) < a.g.VH;
-  const int cb = active ? (tid >> 1) : a.g.VH - 1;
+  const bool active = a.cb0 + (tid >> 1) < a.cb1;
+  const int cb = active ? a.cb0 + (tid >> 1) : a.cb1 - 1;
   double nrm = hop2_site<NFT, REAL, R, EP, LE>(a, cb, tid & 1, active);
   if (a.red) block_partial<R>(nrm, a.red);
 }

@@ -63,9 +63,9 @@ __global__ void __launch_bounds__(HOP_THREADS) k_hop_async(HopArgs<R> a) {
   const Geo g = a.g;
   if (a.stop && *a.stop) return;
   const int tid = threadIdx.x;
-  const int cb0 = blockIdx.x * blockDim.x + tid;
-  const bool active = cb0 < g.VH;
-  const int cb = active ? cb0 : g.VH - 1;
+  const int cs = a.cb0 + blockIdx.x * blockDim.x + tid;
+  const bool active = cs < a.cb1;
+  const int cb = active ? cs : a.cb1 - 1;
   const int outp = a.outp, inp = outp ^ 1;
   int t, x, y, z;
   cb_to_coords(g, cb, outp, t, x, y, z);

@@ -30,7 +30,8 @@ int launch_ep_variant(HopArgs<R> &a, int variant) {
   // variants: 0 one thread per site, 1 two threads per site (spin split),
   // 2 and 3 the same with the register budget capped for 4 resident blocks per SM,
   // 4 one thread per site with the per-direction loads pipelined through shared memory
-  const long threads = (variant & 1) ? 2L * L.VH : L.VH;
+  const long nsites = a.cb1 - a.cb0;
+  const long threads = (variant & 1) ? 2L * nsites : nsites;
   dim3 grid((unsigned)((threads + HOP_THREADS - 1) / HOP_THREADS)), block(HOP_THREADS);
   cudaStream_t s = L.stream;
 #define HOPV(N, RL)                                                                    \
@@ -111,6 +112,11 @@ int launch_ep(HopArgs<R> &a) {
       return HRGPU_E_NF;
     }
     return rc;
+  }
+  if (v < 0 && (a.cb0 != 0 || a.cb1 != L.VH)) {
+    // a launch over part of the lattice is no measure for the full operator:
+    // run the default variant and leave tuning to the first full launch
+    return launch_ep_variant<R, EP>(a, 0);
   }
   if (v < 0) {
     float best = 1e30f;

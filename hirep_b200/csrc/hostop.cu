@@ -1,0 +1,355 @@
+// hostop.cu -- an even-odd preconditioned operator applied to a HOST field in
+// HiRep's layout (hrgpu_apply_op_host), with the host<->device copies
+// overlapped with the computation.
+//
+// HiRep calls Dphi_eopre / Cphi_eopre on spinor_fields in host memory
+// (LibHR/Update/Dphi.c:874-907, :1240-1255).  Done as upload, operator,
+// download, the two PCIe copies run one after the other with the GPU idle.
+// Here the even input is copied in K chunks of HiRep's host order on one
+// stream and scattered into the device layout as each chunk lands; the two
+// hops of the operator run on whole time slabs as soon as their inputs are
+// complete (stage 0 on slab t needs input slabs t-1, t, t+1; stage 1 on slab t
+// needs stage 0 on t-1, t, t+1 and the input on t); output chunks are gathered
+// back into host order and copied out on a second stream as soon as every slab
+// they touch is done.  The copy-out of early chunks then overlaps the copy-in
+// of late ones (PCIe is full duplex) and the hops hide under the copies.
+//
+// The chunks are not of equal size: the output that depends on the last input
+// chunk (that chunk and its time neighbours, the first chunk included through
+// the periodic wrap) can only leave after it, so the first two and the last
+// two chunks are half-size, which halves that tail.
+//
+// With pinned host buffers the whole sequence (copies, scatters, hops,
+// gathers and the cross-stream events) is captured once as a CUDA graph and
+// replayed: its chunks cost tens of API calls that the host would otherwise
+// issue while the copies run.  (Kernels that read and write the mapped host
+// buffers directly were measured too: their PCIe traffic slowed the hops
+// running beside them and the pipeline was no faster.)  The graph is cached per (operator, precision,
+// mass, host buffers, chunking, kernel variants, link storage); the data it
+// reads (links, clover blocks) are read at replay, so new gauge fields need
+// no new graph.  Pageable buffers take the eager path.
+//
+// The device layout puts the time coordinate slowest, so a time slab of one
+// parity is one contiguous range of checkerboard indices, [t S, (t+1) S) with
+// S = X Y Z / 2, and a stage on a run of slabs is one launch.  Every site is
+// computed by the same kernel code as in the whole-lattice operator, so the
+// result is bit-identical to upload + operator + download.
+#include <vector>
+
+#include "dirac.cuh"
+
+namespace hrgpu {
+
+struct HostPipe {
+  long VH = -1;  // lattice the plan was made for
+  int T = 0, K = 0, S = 0;
+  std::vector<int> h0;                  // chunk k: even host sites [h0[k], h0[k+1])
+  std::vector<int> last_chunk;          // per slab: the last chunk carrying one of its even sites
+  std::vector<std::vector<int>> slabs;  // per chunk: the slabs its sites lie in
+  cudaStream_t s_in = nullptr, s_out = nullptr, s_cap = nullptr;  // copy-in, copy-out, capture
+  std::vector<cudaEvent_t> ev_in, ev_out;
+  cudaEvent_t ev_go = nullptr, ev_done = nullptr;
+  void *din = nullptr, *dout = nullptr, *stage_in = nullptr, *stage_out = nullptr;
+  size_t field_bytes = 0, stage_bytes = 0;
+};
+static HostPipe HP;
+static int hp_chunks = 10;  // hrgpu_set_host_chunks
+
+struct HostGraph {
+  int clover, g5, prec, K;
+  double mass;
+  const void *hin;
+  void *hout;
+  const void *U;
+  int v0, v1, flt_links;
+  long VH;
+  cudaGraphExec_t exec = nullptr;
+};
+static std::vector<HostGraph> HG;  // a few cached graphs
+constexpr size_t HG_MAX = 8;
+
+static void free_graphs() {
+  for (HostGraph &h : HG)
+    if (h.exec) cudaGraphExecDestroy(h.exec);
+  HG.clear();
+}
+
+static void free_events() {
+  for (cudaEvent_t e : HP.ev_in) cudaEventDestroy(e);
+  for (cudaEvent_t e : HP.ev_out) cudaEventDestroy(e);
+  HP.ev_in.clear();
+  HP.ev_out.clear();
+}
+
+void hostop_release() {
+  free_graphs();
+  free_events();
+  if (HP.ev_go) cudaEventDestroy(HP.ev_go);
+  if (HP.ev_done) cudaEventDestroy(HP.ev_done);
+  if (HP.s_in) cudaStreamDestroy(HP.s_in);
+  if (HP.s_out) cudaStreamDestroy(HP.s_out);
+  if (HP.s_cap) cudaStreamDestroy(HP.s_cap);
+  for (void *p : {HP.din, HP.dout, HP.stage_in, HP.stage_out})
+    if (p) cudaFree(p);
+  HP = HostPipe();
+}
+
+// chunks of the even host sites and the slabs they touch, from HiRep's ipt
+static int make_plan(int K) {
+  const bool fresh = HP.VH != L.VH || HP.K != K;
+  if (!fresh) return 0;
+  free_graphs();  // they wait on the events of the old plan
+  free_events();
+  if (!HP.s_in) {
+    HR_CUDA(cudaStreamCreateWithFlags(&HP.s_in, cudaStreamNonBlocking));
+    HR_CUDA(cudaStreamCreateWithFlags(&HP.s_out, cudaStreamNonBlocking));
+    HR_CUDA(cudaStreamCreateWithFlags(&HP.s_cap, cudaStreamNonBlocking));
+    HR_CUDA(cudaEventCreateWithFlags(&HP.ev_go, cudaEventDisableTiming));
+    HR_CUDA(cudaEventCreateWithFlags(&HP.ev_done, cudaEventDisableTiming));
+  }
+  HP.T = L.T;
+  HP.S = L.X * L.Y * L.Z / 2;
+  HP.K = K;
+  // weights: half-size first two and last two chunks (K >= 6), equal otherwise
+  std::vector<double> w(K, 1.0);
+  if (K >= 6) w[0] = w[1] = w[K - 2] = w[K - 1] = 0.5;
+  double wsum = 0;
+  for (double x : w) wsum += x;
+  HP.h0.assign(K + 1, 0);
+  double acc = 0;
+  for (int k = 0; k < K; k++) {
+    HP.h0[k] = (int)((double)L.VH * acc / wsum);
+    acc += w[k];
+  }
+  HP.h0[K] = (int)L.VH;
+  for (int k = 1; k < K; k++)  // every chunk non-empty (K <= VH)
+    if (HP.h0[k] <= HP.h0[k - 1]) HP.h0[k] = HP.h0[k - 1] + 1;
+  for (int k = 0; k < K; k++)
+    HR_REQUIRE(HP.h0[k] < HP.h0[k + 1], HRGPU_E_ARG, "apply_op_host: %d chunks of %ld sites", K, (long)L.VH);
+  HP.last_chunk.assign(HP.T, -1);
+  HP.slabs.assign(K, {});
+  for (int k = 0; k < K; k++) {
+    std::vector<char> seen(HP.T, 0);
+    for (int ix = HP.h0[k]; ix < HP.h0[k + 1]; ix++) {
+      const int t = L.h_h2d[ix] / HP.S;  // even site: device index = cb
+      if (!seen[t]) {
+        seen[t] = 1;
+        HP.slabs[k].push_back(t);
+      }
+      if (k > HP.last_chunk[t]) HP.last_chunk[t] = k;
+    }
+  }
+  HP.ev_in.resize(K);
+  HP.ev_out.resize(K);
+  for (int k = 0; k < K; k++) {
+    HR_CUDA(cudaEventCreateWithFlags(&HP.ev_in[k], cudaEventDisableTiming));
+    HR_CUDA(cudaEventCreateWithFlags(&HP.ev_out[k], cudaEventDisableTiming));
+  }
+  HP.VH = L.VH;
+  return 0;
+}
+
+static int ensure_buffers(int prec) {
+  const size_t fb = spinor_bytes(HRGPU_EVEN, prec);
+  const size_t sb = (size_t)L.VH * 4 * L.nf * (prec == HRGPU_DOUBLE ? sizeof(double2) : sizeof(float2));
+  if (fb > HP.field_bytes) {
+    free_graphs();  // they hold the old buffers
+    for (void **p : {&HP.din, &HP.dout}) {
+      if (*p) HR_CUDA(cudaFree(*p));
+      *p = nullptr;
+      HR_CUDA(cudaMalloc(p, fb));
+      HR_CUDA(cudaMemsetAsync(*p, 0, fb, L.stream));  // padding sites stay zero
+    }
+    HP.field_bytes = fb;
+  }
+  if (sb > HP.stage_bytes) {
+    free_graphs();
+    for (void **p : {&HP.stage_in, &HP.stage_out}) {
+      if (*p) HR_CUDA(cudaFree(*p));
+      *p = nullptr;
+      HR_CUDA(cudaMalloc(p, sb));
+    }
+    HP.stage_bytes = sb;
+  }
+  return 0;
+}
+
+// run one stage on every slab that is not done and whose inputs are, in runs
+// of consecutive slabs (one launch per run)
+template <typename R, typename Ready>
+static int run_stage(int clover, double mass, int stage, int g5, std::vector<char> &done, Ready ready) {
+  const int T = HP.T;
+  int t = 0;
+  while (t < T) {
+    if (done[t] || !ready(t)) {
+      t++;
+      continue;
+    }
+    int e = t;
+    while (e < T && !done[e] && ready(e)) e++;
+    if (int rc = eo_stage<R>(clover, mass, stage, HRGPU_EVEN, HP.dout, HP.din, g5, nullptr, t * HP.S, e * HP.S))
+      return rc;
+    for (int u = t; u < e; u++) done[u] = 1;
+    t = e;
+  }
+  return 0;
+}
+
+// enqueue the whole pipeline on L.stream (and the two copy streams, joined back
+// into L.stream at the end); nothing here waits on the host
+template <typename R>
+static int enqueue_host(int clover, int g5, double mass, void *host_out, const void *host_in, int prec) {
+  const int K = HP.K;
+  const size_t sb = (size_t)4 * L.nf * sizeof(typename C2<R>::T);  // bytes of one site
+  const int T = HP.T;
+  std::vector<char> in_done(T, 0), d0(T, 0), d1(T, 0), sent(K, 0);
+  auto up = [T](int t) { return (t + T - 1) % T; };
+  auto dn = [T](int t) { return (t + 1) % T; };
+  HR_CUDA(cudaEventRecord(HP.ev_go, L.stream));
+  HR_CUDA(cudaStreamWaitEvent(HP.s_in, HP.ev_go, 0));
+  HR_CUDA(cudaStreamWaitEvent(HP.s_out, HP.ev_go, 0));
+  for (int k = 0; k < K; k++) {
+    const size_t off = (size_t)HP.h0[k] * sb, len = (size_t)(HP.h0[k + 1] - HP.h0[k]) * sb;
+    HR_CUDA(cudaMemcpyAsync((char *)HP.stage_in + off, (const char *)host_in + off, len, cudaMemcpyHostToDevice,
+                            HP.s_in));
+    HR_CUDA(cudaEventRecord(HP.ev_in[k], HP.s_in));
+  }
+  for (int k = 0; k < K; k++) {
+    HR_CUDA(cudaStreamWaitEvent(L.stream, HP.ev_in[k], 0));
+    if (int rc = spinor_scatter_even(HP.din, (const char *)HP.stage_in + (size_t)HP.h0[k] * sb, HP.h0[k],
+                                     HP.h0[k + 1] - HP.h0[k], prec, L.stream))
+      return rc;
+    for (int t = 0; t < T; t++)
+      if (HP.last_chunk[t] == k) in_done[t] = 1;
+    if (int rc = run_stage<R>(clover, mass, 0, g5, d0,
+                              [&](int t) { return in_done[up(t)] && in_done[t] && in_done[dn(t)]; }))
+      return rc;
+    if (int rc = run_stage<R>(clover, mass, 1, g5, d1,
+                              [&](int t) { return d0[up(t)] && d0[t] && d0[dn(t)] && in_done[t]; }))
+      return rc;
+    for (int j = 0; j < K; j++) {
+      if (sent[j]) continue;
+      bool ok = true;
+      for (int t : HP.slabs[j]) ok = ok && d1[t];
+      if (!ok) continue;
+      const int nj = HP.h0[j + 1] - HP.h0[j];
+      const size_t off = (size_t)HP.h0[j] * sb, len = (size_t)nj * sb;
+      if (int rc = spinor_gather_even((char *)HP.stage_out + off, HP.dout, HP.h0[j], nj, prec, L.stream)) return rc;
+      HR_CUDA(cudaEventRecord(HP.ev_out[j], L.stream));
+      HR_CUDA(cudaStreamWaitEvent(HP.s_out, HP.ev_out[j], 0));
+      HR_CUDA(cudaMemcpyAsync((char *)host_out + off, (const char *)HP.stage_out + off, len, cudaMemcpyDeviceToHost,
+                              HP.s_out));
+      sent[j] = 1;
+    }
+  }
+  for (int j = 0; j < K; j++)
+    HR_REQUIRE(sent[j], HRGPU_E_STATE, "apply_op_host: output chunk %d was never complete", j);
+  HR_CUDA(cudaEventRecord(HP.ev_done, HP.s_out));
+  HR_CUDA(cudaStreamWaitEvent(L.stream, HP.ev_done, 0));
+  return 0;
+}
+
+static bool pinned(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+template <typename R>
+static int apply_host(int clover, int g5, double mass, void *host_out, const void *host_in, int prec) {
+  const int K = hp_chunks > (int)L.VH ? (int)L.VH : hp_chunks;
+  if (int rc = make_plan(K)) return rc;
+  if (int rc = ensure_buffers(prec)) return rc;
+  const int pi = sizeof(R) == 8 ? 0 : (L.flt_links == HRGPU_LINKS_BF16 ? 2 : 1);
+  const int e0 = clover ? EP_CLOV_INV : EP_AXPY, e1 = clover ? EP_CLOV : EP_AXPY;
+  // the graph needs the kernel variants settled (the autotuner times launches,
+  // which a capture cannot) and the operator's scratch field allocated
+  const bool settled = L.hop_force >= 0 || (L.hop_variant[pi][e0] >= 0 && L.hop_variant[pi][e1] >= 0);
+  const bool have_tmp = (sizeof(R) == 8 ? L.tmp_o : L.tmp_o_f) != nullptr;
+  if (!(settled && have_tmp && pinned(host_in) && pinned(host_out))) {
+    if (int rc = enqueue_host<R>(clover, g5, mass, host_out, host_in, prec)) return rc;
+  } else {
+    HostGraph key;
+    key.clover = clover;
+    key.g5 = g5;
+    key.prec = prec;
+    key.K = K;
+    key.mass = mass;
+    key.hin = host_in;
+    key.hout = host_out;
+    key.U = sizeof(R) == 8 ? (const void *)L.U : (const void *)L.Uf;
+    key.v0 = L.hop_force >= 0 ? 100 + L.hop_force : L.hop_variant[pi][e0];
+    key.v1 = L.hop_force >= 0 ? 100 + L.hop_force : L.hop_variant[pi][e1];
+    key.flt_links = L.flt_links;
+    key.VH = L.VH;
+    HostGraph *hit = nullptr;
+    for (HostGraph &h : HG)
+      if (h.clover == key.clover && h.g5 == key.g5 && h.prec == key.prec && h.K == key.K && h.mass == key.mass &&
+          h.hin == key.hin && h.hout == key.hout && h.U == key.U && h.v0 == key.v0 && h.v1 == key.v1 &&
+          h.flt_links == key.flt_links && h.VH == key.VH)
+        hit = &h;
+    if (!hit) {
+      if (HG.size() >= HG_MAX) free_graphs();
+      if (sizeof(R) == 4 && L.flt_links == HRGPU_LINKS_BF16)
+        if (int rc = ensure_links_bf16()) return rc;  // not inside the capture
+      // captured on a private stream (the library stream may be the legacy
+      // default stream, which cannot be captured) and replayed into L.stream
+      cudaGraph_t graph = nullptr;
+      cudaStream_t saved = L.stream;
+      HR_CUDA(cudaStreamBeginCapture(HP.s_cap, cudaStreamCaptureModeRelaxed));
+      L.stream = HP.s_cap;
+      int rc = enqueue_host<R>(clover, g5, mass, host_out, host_in, prec);
+      L.stream = saved;
+      cudaError_t ce = cudaStreamEndCapture(HP.s_cap, &graph);
+      if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+      }
+      if (ce != cudaSuccess) return fail_cuda(ce, "apply_op_host capture", __FILE__, __LINE__);
+      ce = cudaGraphInstantiate(&key.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ce != cudaSuccess) return fail_cuda(ce, "apply_op_host instantiate", __FILE__, __LINE__);
+      HG.push_back(key);
+      hit = &HG.back();
+    }
+    HR_CUDA(cudaGraphLaunch(hit->exec, L.stream));
+  }
+  HR_CUDA(cudaStreamSynchronize(L.stream));
+  add_mvm(2);  // the two hops of one application, as the whole-lattice operator counts them
+  return 0;
+}
+
+}  // namespace hrgpu
+
+using namespace hrgpu;
+
+extern "C" {
+
+int hrgpu_set_host_chunks(int chunks) {
+  HR_REQUIRE(chunks >= 1, HRGPU_E_ARG, "set_host_chunks: chunks must be >= 1");
+  hp_chunks = chunks;
+  return 0;
+}
+
+int hrgpu_apply_op_host(int op, double mass, void *host_out, const void *host_in, int prec) {
+  HR_REQUIRE(L.ready, HRGPU_E_STATE, "apply_op_host: lattice not initialised");
+  HR_REQUIRE(host_out && host_in && host_out != host_in, HRGPU_E_ARG, "apply_op_host: bad host fields");
+  HR_REQUIRE(prec == HRGPU_DOUBLE || prec == HRGPU_FLOAT, HRGPU_E_ARG, "apply_op_host: bad precision");
+  HR_REQUIRE(op == HRGPU_OP_DPHI_EOPRE || op == HRGPU_OP_G5DPHI_EOPRE || op == HRGPU_OP_CPHI_EOPRE ||
+                 op == HRGPU_OP_G5CPHI_EOPRE,
+             HRGPU_E_ARG, "apply_op_host: op %d is not an even-odd preconditioned operator (4..7)", op);
+  if (int rc = check_gauge(prec)) return rc;
+  const int clover = op == HRGPU_OP_CPHI_EOPRE || op == HRGPU_OP_G5CPHI_EOPRE;
+  const int g5 = op == HRGPU_OP_G5DPHI_EOPRE || op == HRGPU_OP_G5CPHI_EOPRE;
+  if (clover) {
+    HR_REQUIRE(L.clover, HRGPU_E_STATE, "apply_op_host: no clover term (hrgpu_clover_init)");
+    if (int rc = clover_prepare(mass, prec)) return rc;
+  }
+  return prec == HRGPU_DOUBLE ? apply_host<double>(clover, g5, mass, host_out, host_in, prec)
+                              : apply_host<float>(clover, g5, mass, host_out, host_in, prec);
+}
+
+}  // extern "C"

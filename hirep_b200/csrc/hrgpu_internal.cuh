@@ -133,6 +133,9 @@ int ensure_links_bf16();  // the BF16 copy of the links, made from the FP64 ones
 int compute_clover_term_dev();
 void cg_release();
 int ensure_stage(size_t bytes);
+int spinor_scatter_even(void *dev, const void *stage, int base, int nsites, int prec, cudaStream_t s);
+int spinor_gather_even(void *stage, const void *dev, int base, int nsites, int prec, cudaStream_t s);
+void hostop_release();
 
 // ---------------------------------------------------------------------------
 // small complex helpers

@@ -468,6 +468,37 @@ int hrgpu_lattice_init(int T, int X, int Y, int Z, int ng, int repr, const int *
   return 0;
 }
 
+}  // extern "C"
+
+namespace hrgpu {
+// host-order staging buffer <-> even-parity device field, for the host sites
+// [base, base+nsites) (stage points at host site base)
+int spinor_scatter_even(void *dev, const void *stage, int base, int nsites, int prec, cudaStream_t s) {
+  const int ncomp = 4 * L.nf;
+  const long n = (long)nsites * ncomp;
+  if (n == 0) return 0;
+  if (prec == HRGPU_DOUBLE)
+    k_spinor_in<double2><<<nblk(n), 256, 0, s>>>((double2 *)dev, (const double2 *)stage, L.d_h2d, base, nsites, ncomp, L.ld, 0);
+  else
+    k_spinor_in<float2><<<nblk(n), 256, 0, s>>>((float2 *)dev, (const float2 *)stage, L.d_h2d, base, nsites, ncomp, L.ld, 0);
+  HR_LAUNCH_CHECK();
+  return 0;
+}
+int spinor_gather_even(void *stage, const void *dev, int base, int nsites, int prec, cudaStream_t s) {
+  const int ncomp = 4 * L.nf;
+  const long n = (long)nsites * ncomp;
+  if (n == 0) return 0;
+  if (prec == HRGPU_DOUBLE)
+    k_spinor_out<double2><<<nblk(n), 256, 0, s>>>((double2 *)stage, (const double2 *)dev, L.d_h2d, base, nsites, ncomp, L.ld, 0);
+  else
+    k_spinor_out<float2><<<nblk(n), 256, 0, s>>>((float2 *)stage, (const float2 *)dev, L.d_h2d, base, nsites, ncomp, L.ld, 0);
+  HR_LAUNCH_CHECK();
+  return 0;
+}
+}  // namespace hrgpu
+
+extern "C" {
+
 int hrgpu_spinor_upload(void *dev, const void *host, int par, int prec) {
   HR_REQUIRE(L.ready, HRGPU_E_STATE, "hrgpu_spinor_upload: lattice not initialised");
   HR_REQUIRE(dev && host && par >= 0 && par <= 2 && (prec == 0 || prec == 1), HRGPU_E_ARG, "hrgpu_spinor_upload: bad arguments");

@@ -399,6 +399,22 @@ class Lattice:
             b.pack(fields)
         return b
 
+    def apply_op_host(self, op, mass, host_in, prec=DOUBLE, out=None):
+        """An even-odd operator (OP_DPHI_EOPRE .. OP_G5CPHI_EOPRE) on an even host
+        field [VH][4][NF] in HiRep order; the copies overlap the computation.
+        host_in / out may be pinned torch tensors viewed as numpy (the fast path)
+        or plain numpy arrays."""
+        dt = np.complex128 if prec == DOUBLE else np.complex64
+        host_in = np.ascontiguousarray(host_in, dt)
+        assert host_in.shape == (self.VH, 4, self.nf), host_in.shape
+        if out is None:
+            out = np.empty_like(host_in)
+        _check(self.L.hrgpu_apply_op_host(op, D(mass), _ptr(out), _ptr(host_in), prec), "apply_op_host")
+        return out
+
+    def set_host_chunks(self, chunks):
+        _check(self.L.hrgpu_set_host_chunks(chunks), "set_host_chunks")
+
     def apply_op_batch(self, op, mass, out, inp):
         _check(self.L.hrgpu_apply_op_batch(op, out.prec, D(mass), out.ptr, inp.ptr, out.nb), "apply_op_batch")
 

@@ -166,6 +166,18 @@ int hrgpu_H2(void *out, const void *in);
 int hrgpu_H(void *out, const void *in);
 int hrgpu_D(void *out, const void *in);
 
+/* ------------------------------------------------------------ host fields -- */
+/* An even-odd preconditioned operator (op 4..7: Dphi_eopre, g5Dphi_eopre,
+ * Cphi_eopre, g5Cphi_eopre; Dphi.c:874-985, :1240-1261) applied to an even host
+ * field in HiRep's layout ([VH][4][NF] complex in ipt order, complex128 for
+ * HRGPU_DOUBLE, complex64 for HRGPU_FLOAT), result written to host_out.  The
+ * field is moved in chunks whose copies overlap the hops on the time slabs
+ * already complete (bit-identical to upload + operator + download).  Host
+ * buffers should be pinned (cudaHostAlloc / cudaHostRegister) for the copies to
+ * overlap. */
+int hrgpu_apply_op_host(int op, double mass, void *host_out, const void *host_in, int prec);
+int hrgpu_set_host_chunks(int chunks); /* chunks of the pipeline (default 10; 1 = no overlap) */
+
 /* ---------------------------------------------------------------- clover -- */
 int hrgpu_clover_init(double csw);                  /* clover_init, clover_tools.c:360-373        */
 /* the same with the exponential clover term of WITH_EXPCLOVER (Dphi.c:1292-1482,
