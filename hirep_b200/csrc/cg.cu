@@ -8,8 +8,8 @@
 //   M k (the fused hopping kernels) -> <k,Mk> partials -> fold_alpha ->
 //   update1 (x_i += c_i p_i, r += omega Mk, |r|^2 partials) -> fold_lambda ->
 //   update2 (k = gamma k + r, p_i = d_i p_i + z3_i r) -> advance
-// The host launches several iterations at a time and reads one state word
-// between chunks.  When fold_lambda finds the stopping condition it marks the
+// The host launches several iterations at a time (a captured CUDA graph) and
+// reads one state word between chunks.  When fold_lambda finds the stopping condition it marks the
 // state; the remaining kernels of that iteration finish it exactly as HiRep's
 // loop body would, and every kernel of later iterations returns at once, so the
 // solution and the iteration count are those of HiRep's loop.
@@ -226,6 +226,30 @@ static int cg_workspace(int prec, int nvec, size_t bytes) {
   return 0;
 }
 
+// The chunk of iterations as a CUDA graph, captured once per (operator, mass,
+// work buffers, kernel variants, link storage) and replayed: ten launches per
+// iteration, most of them small, cost more in launch gaps than in work.  The
+// graph reads the links and clover blocks at replay; the clover blocks (for
+// this mass) and the BF16 link copy are brought up to date before each replay.
+// (Folding the partials in the last block of the kernel that wrote them, with
+// an atomic ticket, instead of one-block fold kernels was measured slower: the
+// per-block fence outweighs the launches it saves inside a graph.)
+struct CGGraph {
+  int op = -1;
+  double mass = 0;
+  const void *ptrs[10] = {};
+  int v[3] = {-1, -1, -1}, force = -1, flt_links = -1;
+  unsigned long mvm = 0;  // hop launches in one replay (the MVM counter)
+  cudaGraphExec_t exec = nullptr;
+};
+static CGGraph CGG[2];  // [prec]
+static cudaStream_t cg_cap = nullptr;
+
+static void drop_cg_graph(CGGraph &c) {
+  if (c.exec) cudaGraphExecDestroy(c.exec);
+  c = CGGraph();
+}
+
 void cg_release() {
   batch_release();
   qmr_release();
@@ -234,6 +258,9 @@ void cg_release() {
   cudaFree(FW.dres); cudaFree(FW.dres2); cudaFree(FW.dtmp);
   for (void *b : FW.fbuf) cudaFree(b);
   FW = FltWork();
+  for (int q = 0; q < 2; q++) drop_cg_graph(CGG[q]);
+  if (cg_cap) cudaStreamDestroy(cg_cap);
+  cg_cap = nullptr;
   for (int q = 0; q < 2; q++) {
     for (void *b : W[q].bufs) cudaFree(b);
     W[q].bufs.clear();
@@ -250,6 +277,87 @@ void cg_release() {
 static unsigned red_grid(long n) {
   long b = (n + RED_THREADS - 1) / RED_THREADS;
   return (unsigned)(b < RED_MAX_BLOCKS ? b : RED_MAX_BLOCKS);
+}
+
+// CG_CHUNK iterations, launched one kernel at a time
+template <typename R>
+static int cg_iterations(int op, int prec, double mass, CGWork &w, void *k, void *r, void *Mk, long ne, unsigned g) {
+  typedef typename C2<R>::T V;
+  V *const *dx = (V *const *)w.d_ptrs;
+  V *const *dp = (V *const *)(w.d_ptrs + MAXS);
+  for (int c = 0; c < CG_CHUNK; c++) {
+    if (int rc = apply_op(op, prec, mass, Mk, k)) return rc;
+    k_cg_dot<V><<<g, RED_THREADS, 0, L.stream>>>(w.S, (const V *)k, (const V *)Mk, ne, L.partials);
+    k_cg_fold_alpha<<<1, RED_THREADS, 0, L.stream>>>(w.S, L.partials, g);
+    k_cg_update1<V><<<g, RED_THREADS, 0, L.stream>>>(w.S, dx, dp, (V *)r, (const V *)Mk, ne, L.partials);
+    k_cg_fold_lambda<<<1, RED_THREADS, 0, L.stream>>>(w.S, L.partials, g);
+    k_cg_update2<V><<<g, RED_THREADS, 0, L.stream>>>(w.S, dp, (V *)k, (const V *)r, ne);
+    k_cg_advance<<<1, 1, 0, L.stream>>>(w.S);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "cg iteration", __FILE__, __LINE__);
+  }
+  return 0;
+}
+static bool op_is_clover(int op) {
+  return op == HRGPU_OP_G5CPHI_EOPRE_SQ || op == HRGPU_OP_G5CPHI_SQ || op == HRGPU_OP_CPHI_EOPRE ||
+         op == HRGPU_OP_G5CPHI_EOPRE || op == HRGPU_OP_CPHI;
+}
+template <typename R>
+static int cg_chunk(int op, int prec, double mass, CGWork &w, void *k, void *r, void *Mk, long ne, unsigned g) {
+  if (op_is_clover(op))
+    if (int rc = clover_prepare(mass, prec)) return rc;
+  if (prec == HRGPU_FLOAT && L.flt_links == HRGPU_LINKS_BF16)
+    if (int rc = ensure_links_bf16()) return rc;
+  const int pi = prec == HRGPU_DOUBLE ? 0 : (L.flt_links == HRGPU_LINKS_BF16 ? 2 : 1);
+  const bool clover = op_is_clover(op);
+  const bool settled = L.hop_force >= 0 || (clover ? (L.hop_variant[pi][EP_CLOV] >= 0 &&
+                                                      (op == HRGPU_OP_G5CPHI_SQ || op == HRGPU_OP_CPHI ||
+                                                       L.hop_variant[pi][EP_CLOV_INV] >= 0))
+                                                   : L.hop_variant[pi][EP_AXPY] >= 0);
+  if (!settled) return cg_iterations<R>(op, prec, mass, w, k, r, Mk, ne, g);  // tunes the hopping kernels
+  const void *links = prec == HRGPU_DOUBLE ? (const void *)L.U
+                                           : (L.flt_links == HRGPU_LINKS_BF16 ? (const void *)L.Ubf : (const void *)L.Uf);
+  const void *ptrs[10] = {k, r, Mk, w.S, w.d_ptrs, L.partials, links, L.cur_stop,
+                          prec == HRGPU_DOUBLE ? L.tmp_e : L.tmp_e_f, prec == HRGPU_DOUBLE ? L.tmp_o : L.tmp_o_f};
+  CGGraph &c = CGG[prec];
+  bool same = c.exec && c.op == op && c.mass == mass && c.force == L.hop_force && c.flt_links == L.flt_links;
+  for (int i = 0; i < 3 && same; i++) same = c.v[i] == L.hop_variant[pi][i];
+  for (int i = 0; i < 10 && same; i++) same = c.ptrs[i] == ptrs[i];
+  if (!same) {
+    drop_cg_graph(c);
+    if (!cg_cap) HR_CUDA(cudaStreamCreateWithFlags(&cg_cap, cudaStreamNonBlocking));
+    const unsigned long m0 = mvm_count();
+    cudaGraph_t graph = nullptr;
+    cudaStream_t saved = L.stream;
+    HR_CUDA(cudaStreamBeginCapture(cg_cap, cudaStreamCaptureModeRelaxed));
+    L.stream = cg_cap;
+    int rc = cg_iterations<R>(op, prec, mass, w, k, r, Mk, ne, g);
+    L.stream = saved;
+    cudaError_t e = cudaStreamEndCapture(cg_cap, &graph);
+    const unsigned long dm = mvm_count() - m0;
+    mvm_restore(m0);  // nothing ran yet
+    if (rc) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    if (e != cudaSuccess) return fail_cuda(e, "cg capture", __FILE__, __LINE__);
+    e = cudaGraphInstantiate(&c.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      c.exec = nullptr;
+      return fail_cuda(e, "cg graph instantiate", __FILE__, __LINE__);
+    }
+    c.op = op;
+    c.mass = mass;
+    c.force = L.hop_force;
+    c.flt_links = L.flt_links;
+    for (int i = 0; i < 3; i++) c.v[i] = L.hop_variant[pi][i];
+    for (int i = 0; i < 10; i++) c.ptrs[i] = ptrs[i];
+    c.mvm = dm;
+  }
+  HR_CUDA(cudaGraphLaunch(c.exec, L.stream));
+  add_mvm(c.mvm);
+  return 0;
 }
 
 // cg_mshift_core (cg_mshift.c:24-145) / cg_mshift_flt_core (cg_mshift_flt.c:22-140).
@@ -310,24 +418,11 @@ static int cg_core(int op, double mass, int n, const double *shift, double err2,
     ptrs[MAXS + i] = w.bufs[i];
   }
   HR_CUDA(cudaMemcpyAsync(w.d_ptrs, ptrs, sizeof(void *) * 2 * MAXS, cudaMemcpyHostToDevice, L.stream));
-  V *const *dx = (V *const *)w.d_ptrs;
-  V *const *dp = (V *const *)(w.d_ptrs + MAXS);
   const unsigned g = red_grid(ne);
   L.cur_stop = &w.S->state;
   int rc = 0;
   for (;;) {
-    for (int c = 0; c < CG_CHUNK && rc == 0; c++) {
-      rc = apply_op(op, prec, mass, Mk, k);
-      if (rc) break;
-      k_cg_dot<V><<<g, RED_THREADS, 0, L.stream>>>(w.S, (const V *)k, (const V *)Mk, ne, L.partials);
-      k_cg_fold_alpha<<<1, RED_THREADS, 0, L.stream>>>(w.S, L.partials, g);
-      k_cg_update1<V><<<g, RED_THREADS, 0, L.stream>>>(w.S, dx, dp, (V *)r, (const V *)Mk, ne, L.partials);
-      k_cg_fold_lambda<<<1, RED_THREADS, 0, L.stream>>>(w.S, L.partials, g);
-      k_cg_update2<V><<<g, RED_THREADS, 0, L.stream>>>(w.S, dp, (V *)k, (const V *)r, ne);
-      k_cg_advance<<<1, 1, 0, L.stream>>>(w.S);
-      cudaError_t e = cudaGetLastError();
-      if (e != cudaSuccess) rc = fail_cuda(e, "cg iteration", __FILE__, __LINE__);
-    }
+    rc = cg_chunk<R>(op, prec, mass, w, k, r, Mk, ne, g);
     if (rc) break;
     cudaError_t e = cudaMemcpyAsync(&h, w.S, sizeof(CGState), cudaMemcpyDeviceToHost, L.stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(L.stream);

@@ -231,6 +231,8 @@ int op_parity(int op) {
 double static_mass() { return g_static_mass; }
 
 void add_mvm(unsigned long n) { g_mvm += n; }
+unsigned long mvm_count() { return g_mvm; }
+void mvm_restore(unsigned long n) { g_mvm = n; }
 
 }  // namespace hrgpu
 

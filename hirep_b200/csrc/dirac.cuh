@@ -24,6 +24,8 @@ int apply_op(int op, int prec, double mass, void *out, const void *in);
 int op_parity(int op);
 double static_mass();
 void add_mvm(unsigned long n);  // hops done outside hop(), e.g. replayed CUDA graphs
+unsigned long mvm_count();      // the raw hop counter (captures read and restore it)
+void mvm_restore(unsigned long n);
 void batch_release();           // batch.cu: workspaces and captured graphs
 void qmr_release();             // qmr.cu: the g5QMR / MINRES work fields
 void hmc_release();             // hmc.cu: generators, local action
