@@ -127,9 +127,10 @@ __global__ void k_clover_pack_diag(const double2 *cl, double sigma, double *dg, 
   }
 }
 
-// LDL (clover_tools.c:97-114) and explicit inverse, packed
+// LDL (clover_tools.c:97-114) and explicit inverse, packed; ldet: the product
+// of the LDL diagonals of both blocks (det D_oo, for clover_la_logdet)
 template <int N>
-__global__ void k_clover_pack_inv(const double2 *cl, double sigma, double *dg, double2 *od, Geo g) {
+__global__ void k_clover_pack_inv(const double2 *cl, double sigma, double *dg, double2 *od, double *ldet, Geo g) {
   long d = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (d >= 2L * g.ld) return;
   int p = d >= g.ld ? 1 : 0;
@@ -140,8 +141,10 @@ __global__ void k_clover_pack_inv(const double2 *cl, double sigma, double *dg, d
       for (int i = 0; i < n; i++) dg[((long)b * n + i) * lp + d] = 0.0;
       for (int k = 0; k < N * (2 * N - 1); k++) od[((long)b * N * (2 * N - 1) + k) * lp + d] = make_double2(0.0, 0.0);
     }
+    ldet[d] = 1.0;
     return;
   }
+  double prod = 1.0;
   double2 A[n * (n + 1) / 2];
   double2 col[n];
 #define CP(i, j) A[(i) * ((i) + 1) / 2 + (j)]
@@ -165,6 +168,7 @@ __global__ void k_clover_pack_inv(const double2 *cl, double sigma, double *dg, d
         CP(j, i) = make_double2(CP(j, i).x / di, CP(j, i).y / di);
       }
     }
+    for (int i = 0; i < n; i++) prod *= CP(i, i).x;
     for (int c = 0; c < n; c++) {
       for (int i = 0; i < n; i++) col[i] = make_double2(i == c ? 1.0 : 0.0, 0.0);
       for (int i = c; i < n; i++)
@@ -184,6 +188,7 @@ __global__ void k_clover_pack_inv(const double2 *cl, double sigma, double *dg, d
       for (int i = c + 1; i < n; i++) od[((long)b * N * (2 * N - 1) + i * (i - 1) / 2 + c) * lp + d] = col[i];
     }
   }
+  ldet[d] = prod;
 #undef CP
 }
 
@@ -307,6 +312,7 @@ static int alloc_clover() {
     HR_CUDA(cudaMalloc(&L.cl_idg_f, sizeof(float) * 2 * n * lp));
     HR_CUDA(cudaMalloc(&L.cl_iod_f, sizeof(float2) * 2 * no * lp));
     HR_CUDA(cudaMalloc(&L.cl_force, sizeof(double2) * 6 * n2 * lp));
+    HR_CUDA(cudaMalloc(&L.cl_ldet, sizeof(double) * lp));
     HR_CUDA(cudaMemsetAsync(L.cl_force, 0, sizeof(double2) * 6 * n2 * lp, L.stream));
   }
   return 0;
@@ -343,7 +349,7 @@ int clover_prepare(double mass, int prec) {
     L.clover_gen[HRGPU_DOUBLE]++;
   }
   if (L.sigma != sigma) {
-    HR_NFC_DISPATCH(L.nf, (k_clover_pack_inv<N_><<<nb(n, 64), 64, 0, L.stream>>>(L.cl_term, sigma, L.cl_idg, L.cl_iod, g)));
+    HR_NFC_DISPATCH(L.nf, (k_clover_pack_inv<N_><<<nb(n, 64), 64, 0, L.stream>>>(L.cl_term, sigma, L.cl_idg, L.cl_iod, L.cl_ldet, g)));
     HR_LAUNCH_CHECK();
     L.sigma = sigma;
     L.clover_gen[HRGPU_DOUBLE]++;

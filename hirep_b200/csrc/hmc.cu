@@ -238,6 +238,13 @@ __global__ void k_local_action(double *loc, const double *mom, const double2 *Ug
 }
 
 // loc(x) += |pf(x)|^2 for a parity (or full) field
+__global__ void k_clover_la_logdet(double *loc, const double *ldet, double nf, Geo g) {
+  const long cb = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (cb >= g.VH) return;
+  const long d = g.ld + cb;  // odd site
+  loc[d] -= nf * log(ldet[d]);
+}
+
 __global__ void k_pf_local_action(double *loc, const double2 *pf, int par, int nf, Geo g) {
   const long d = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const long nsites = (par == HRGPU_FULL ? 2L : 1L) * g.ld;
@@ -382,6 +389,21 @@ static int sum_sites(const double *v, double *sum) {
   k_sum_partials<<<(unsigned)b, RED_THREADS, 0, L.stream>>>(v, n, L.partials);
   HR_LAUNCH_CHECK();
   return finish_reduction((int)b, 1, sum);
+}
+
+// clover_la_logdet (clover_tools.c:312-331): loc -= nf log det D_oo on the odd
+// sites, det D_oo the product of the LDL diagonals of the two chiral blocks of
+// (4+m) + A at the mass given
+int hrgpu_clover_la_logdet(double nf, double mass) {
+  HR_REQUIRE(L.ready && g_loc, HRGPU_E_STATE, "clover_la_logdet: call hrgpu_local_hmc_action first");
+  HR_REQUIRE(L.clover, HRGPU_E_STATE, "clover_la_logdet: no clover term");
+  HR_REQUIRE(!L.expclover, HRGPU_E_STATE,
+             "clover_la_logdet: the exponential clover term has no log-det term (its blocks are traceless)");
+  if (int rc = clover_prepare(mass, HRGPU_DOUBLE)) return rc;
+  const Geo g = make_geo();
+  k_clover_la_logdet<<<nb128(g.VH), 128, 0, L.stream>>>(g_loc, L.cl_ldet, nf, g);
+  HR_LAUNCH_CHECK();
+  return 0;
 }
 
 int hrgpu_local_action_sum(double *sum) {

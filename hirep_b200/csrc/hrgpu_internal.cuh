@@ -75,6 +75,7 @@ struct Lattice {
   double *cl_dg = nullptr;        // (4+m)+A packed: diag [2][2nf][2*ld]
   double2 *cl_od = nullptr;       //                 off  [2][nf(2nf-1)][2*ld]
   double *cl_idg = nullptr;       // inverse, same packing
+  double *cl_ldet = nullptr;      // [2ld] product of the LDL diagonals of both blocks (det D_oo)
   double2 *cl_iod = nullptr;
   float *cl_dg_f = nullptr, *cl_idg_f = nullptr;
   float2 *cl_od_f = nullptr, *cl_iod_f = nullptr;

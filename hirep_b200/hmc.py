@@ -4,10 +4,13 @@ update_ghmc (LibHR/Update/update_mt.c:148-260) with two monomials: the
 plaquette gauge action (mon_pg.c; force0.c) and an Nf = 2 Wilson pseudofermion
 on the even sites (mon_hmc.c; force_hmc.c, UPDATE_EO branch), integrated with
 the second-order Omelyan integrator (integrators.c:64-93, lambda =
-0.1931833275037836).  With the exponential clover term (WITH_EXPCLOVER) the
-fermion operator is Cphi_eopre (D_update.c:26-95) and the monomial has no
-log-det term (the blocks are traceless, det D_oo is constant); the clover
-force is part of force_fermion_core.  Links, momenta and pseudofermions stay on the device; the
+0.1931833275037836).  With a clover term the fermion operator is Cphi_eopre
+(D_update.c:26-95) and the clover force is part of force_fermion_core.  The
+standard clover monomial also carries the log-det terms of WITH_CLOVER_EO:
+clover_la_logdet(2, m) in its local action (mon_hmc.c:60-67) and
+force_clover_logdet(m, 2) in its force (force_hmc.c:185-190, logdet = 1 as
+mon_hmc.c:109 sets it); the exponential clover term (WITH_EXPCLOVER) has none
+(its blocks are traceless, det D_oo is constant).  Links, momenta and pseudofermions stay on the device; the
 host only holds the scalars of the recursion and the random numbers.
 
 The force solves are either HiRep's (two g5QMR solves on D) or, as the
@@ -27,15 +30,13 @@ LAMBDA_O2MN = 0.1931833275037836
 class HMC:
     def __init__(self, lat, beta, mass, tau, nsteps, force_err2=1e-20, mt_err2=1e-28, force_solver="cg_mixed",
                  bc_t_antiperiodic=True):
-        if lat.csw is not None and not lat.expclover:
-            # the standard clover monomial also needs force_clover_logdet and clover_la_logdet
-            raise NotImplementedError("HMC driver: Wilson or exponential clover fermions (no clover log-det terms)")
         if force_solver not in ("cg_mixed", "cg", "g5qmr"):
             raise ValueError("force_solver: cg_mixed, cg or g5qmr")
         self.lat, self.beta, self.mass, self.tau, self.nsteps = lat, beta, mass, tau, nsteps
         self.force_err2, self.mt_err2, self.force_solver = force_err2, mt_err2, force_solver
         self.bc = bc_t_antiperiodic
         clover = lat.csw is not None
+        self.logdet = clover and not lat.expclover
         self.op_d = G.OP_CPHI_EOPRE if clover else G.OP_DPHI_EOPRE
         self.op_h2 = G.OP_G5CPHI_EOPRE_SQ if clover else G.OP_G5DPHI_EOPRE_SQ
         self.apply_h = lat.g5Cphi_eopre if clover else lat.g5Dphi_eopre
@@ -80,6 +81,8 @@ class HMC:
         self._even_into_full(self.Ys, Y)
         lat.fermion_force_begin()
         lat.force_fermion_core(self.Xs, self.Ys, 1, dt, 1.0)
+        if self.logdet:
+            lat.force_clover_logdet(self.mass, 2.0)  # 2 flavours
         lat.fermion_force_end_momenta(dt)
         self.nforce += 1
 
@@ -117,6 +120,8 @@ class HMC:
         eta = lat.field(G.EVEN, host=eta_h)
         lat.local_hmc_action(False, self.beta)
         lat.pf_local_action(eta)
+        if self.logdet:
+            lat.clover_la_logdet(2.0, self.mass)
         self.apply_h(self.mass, self.pf, eta)  # correct_pf: pf = H eta
         lat.la("zero", self.y)
         self.iters = 0
@@ -132,6 +137,8 @@ class HMC:
             raise G.HRGPUError("HMC: accept/reject solve did not converge")
         lat.local_hmc_action(True, self.beta)
         lat.pf_local_action(self.pf)
+        if self.logdet:
+            lat.clover_la_logdet(2.0, self.mass)
         dH = lat.local_action_sum()
         lat.sync()
         t1 = time.perf_counter()

@@ -364,6 +364,9 @@ class Lattice:
     def pf_local_action(self, pf):
         _check(self.L.hrgpu_pf_local_action(pf.ptr, pf.par), "pf_local_action")
 
+    def clover_la_logdet(self, nf, mass):
+        _check(self.L.hrgpu_clover_la_logdet(D(nf), D(mass)), "clover_la_logdet")
+
     def local_action_sum(self):
         s = ctypes.c_double()
         _check(self.L.hrgpu_local_action_sum(ctypes.byref(s)), "local_action_sum")

@@ -300,6 +300,10 @@ int hrgpu_project_gauge_field(void);
 enum { HRGPU_ACTION_NEW = 0, HRGPU_ACTION_DELTA = 1 };
 int hrgpu_local_hmc_action(int type, double beta);
 int hrgpu_pf_local_action(const void *pf, int par);
+/* clover_la_logdet (clover_tools.c:312-331): local action -= nf log det D_oo on
+ * the odd sites (the standard clover monomial's log-det term; refused for the
+ * exponential clover term, whose det D_oo is constant) */
+int hrgpu_clover_la_logdet(double nf, double mass);
 int hrgpu_local_action_sum(double *sum);
 int hrgpu_local_action_get(double *host);
 /* avr_plaquette (LibHR/Observables/avr_plaquette.c): mean of Re Tr P / NG */

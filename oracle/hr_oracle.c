@@ -2223,6 +2223,20 @@ void orc_force_fermion_core(cplx *Xs, cplx *Ys, int auto_fill_odd, double dt, do
   }
 }
 
+/* clover_la_logdet (clover_tools.c:312-331): la[id] -= nf log(prod of the LDL
+ * diagonals of both blocks) on the odd sites, la in HiRep's site order */
+void orc_clover_la_logdet(double nf, double mass, double *la)
+{
+  orc_compute_ldl_decomp(4.0 + mass);
+  for (int id = VH_; id < V_; id++)
+  {
+    const cplx *A = cl_ldl_ + (size_t)id * 2 * LDLN, *B = A + LDLN;
+    double prod = 1;
+    for (int n = 0; n < 2 * NF_; n++) prod *= creal(CPX(A, n, n)) * creal(CPX(B, n, n));
+    la[id] -= nf * log(prod);
+  }
+}
+
 /* _compute_clover_force + compute_force_logdet (clover_tools.c:208-310) */
 void orc_force_clover_logdet(double mass, double coeff)
 {

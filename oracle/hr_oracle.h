@@ -120,6 +120,7 @@ void orc_mre_guess(int op, int max, const double complex *s, double complex *out
 /* force (LibHR/Update/force_fermion_core.c) */
 void orc_fermion_force_begin(void);
 void orc_force_fermion_core(double complex *Xs, double complex *Ys, int auto_fill_odd, double dt, double residue);
+void orc_clover_la_logdet(double nf, double mass, double *la);
 void orc_force_clover_logdet(double mass, double residue);
 void orc_fermion_force_end(double dt, double *force);
 void orc_get_force_sum(double *f);

@@ -332,6 +332,12 @@ class Oracle:
         self.L.orc_force_fermion_core(_p(Xs), _p(Ys), int(auto_fill_odd), ctypes.c_double(dt), ctypes.c_double(residue))
         return Xs, Ys
 
+    def clover_la_logdet(self, nf, mass, la):
+        """la (per site, HiRep order) -= nf log det D_oo on the odd sites."""
+        la = np.ascontiguousarray(la, np.float64)
+        self.L.orc_clover_la_logdet(ctypes.c_double(nf), ctypes.c_double(mass), _p(la))
+        return la
+
     def force_clover_logdet(self, mass, residue):
         self.L.orc_force_clover_logdet(ctypes.c_double(mass), ctypes.c_double(residue))
 

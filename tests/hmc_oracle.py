@@ -1,6 +1,7 @@
 """An HMC trajectory driven entirely by the oracle: update_ghmc
 (LibHR/Update/update_mt.c:148-260) with the plaquette monomial and an Nf=2
-Wilson or exponential clover pseudofermion on the even sites, O2MN integration
+Wilson, clover (with its log-det terms) or exponential clover pseudofermion on
+the even sites, O2MN integration
 (integrators.c:64-93).  Test infrastructure: the GPU driver's trajectories are
 checked against it, and its own dH ~ dt^2 pins the oracle's forces."""
 import numpy as np
@@ -8,7 +9,7 @@ import numpy as np
 import oracle as O
 
 
-def oracle_trajectory(o, u0, beta, mass, tau, nsteps, rng, force_err2, mt_err2, expclover_csw=None):
+def oracle_trajectory(o, u0, beta, mass, tau, nsteps, rng, force_err2, mt_err2, expclover_csw=None, clover_csw=None):
     """update_ghmc with the plaquette and Nf=2 Wilson (or exponential clover)
     monomials and O2MN, every piece from the oracle (the same random numbers as
     hirep_b200.hmc.HMC.trajectory)."""
@@ -16,9 +17,12 @@ def oracle_trajectory(o, u0, beta, mass, tau, nsteps, rng, force_err2, mt_err2, 
     V, VH, nf, dimg = o.V, o.VH, o.nf, o.dimg
     g5 = np.array([1, 1, -1, -1])[None, :, None]
     keep = {}
-    clover = expclover_csw is not None
-    if clover:
+    clover = expclover_csw is not None or clover_csw is not None
+    logdet = clover_csw is not None  # the standard clover monomial's log-det terms
+    if expclover_csw is not None:
         o.expclover_init(expclover_csw)
+    elif clover_csw is not None:
+        o.clover_init(clover_csw)
     op_h2 = O.OP_G5CPHI_EOPRE_SQ if clover else O.OP_G5DPHI_EOPRE_SQ
     op_d = O.OP_CPHI_EOPRE if clover else O.OP_DPHI_EOPRE
     apply_h = o.g5Cphi_eopre if clover else o.g5Dphi_eopre
@@ -34,7 +38,10 @@ def oracle_trajectory(o, u0, beta, mass, tau, nsteps, rng, force_err2, mt_err2, 
     o.set_mass(mass)
     mom = rng.standard_normal((V, 4, dimg)) / np.sqrt(0.5)
     eta = (rng.standard_normal((VH, 4, nf)) + 1j * rng.standard_normal((VH, 4, nf))) / np.sqrt(2)
-    H0 = o.local_hmc_action(beta, u, mom).sum() + np.sum(np.abs(eta) ** 2)
+    def logdet_action():
+        return o.clover_la_logdet(2.0, mass, np.zeros(V)).sum() if logdet else 0.0
+
+    H0 = o.local_hmc_action(beta, u, mom).sum() + np.sum(np.abs(eta) ** 2) + logdet_action()
     pf = apply_h(mass, eta)
     st = {"y": np.zeros_like(eta), "count": 0, "u": u, "mom": mom}
 
@@ -48,6 +55,8 @@ def oracle_trajectory(o, u0, beta, mass, tau, nsteps, rng, force_err2, mt_err2, 
         Xs[:VH], Ys[:VH] = x, st["y"]
         o.fermion_force_begin()
         o.force_fermion_core(Xs, Ys, 1, dt, 1.0)
+        if logdet:
+            o.force_clover_logdet(mass, 2.0)
         st["mom"] = o.fermion_force_end(dt, st["mom"])
 
     def field(dt):
@@ -69,5 +78,5 @@ def oracle_trajectory(o, u0, beta, mass, tau, nsteps, rng, force_err2, mt_err2, 
     st["u"] = o.project_gauge_field(st["u"])
     represent(st["u"])
     xo, _ = o.g5QMR_mshift(op_d, [0.0], mt_err2, g5 * pf)
-    H1 = o.local_hmc_action(beta, st["u"], st["mom"]).sum() + np.sum(np.abs(xo[0]) ** 2)
+    H1 = o.local_hmc_action(beta, st["u"], st["mom"]).sum() + np.sum(np.abs(xo[0]) ** 2) + logdet_action()
     return H1 - H0, st["u"]

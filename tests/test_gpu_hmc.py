@@ -134,6 +134,44 @@ def test_hmc_expclover_trajectory_matches_oracle_trajectory():
     assert np.abs(lat.gauge_get() - u_o).max() < 1e-10
 
 
+def test_clover_la_logdet_matches_oracle():
+    """The standard clover monomial's log-det local action (clover_tools.c:312-331)."""
+    o, lat, u, mom = setup(3, O.SYM, seed=6, eps=0.3)
+    m, csw = -0.3, 1.1
+    o.clover_init(csw)
+    o.compute_clover_term()
+    lat.clover_init(csw)
+    lat.local_hmc_action(False, 5.6)
+    lat.clover_la_logdet(2.0, m)
+    la_o = o.clover_la_logdet(2.0, m, o.local_hmc_action(5.6, u, mom))
+    la_g = lat.local_action()
+    assert np.abs(la_g - la_o).max() < 1e-12 * np.abs(la_o).max()
+    lat.expclover_init(csw)
+    with pytest.raises(G.HRGPUError, match="no log-det term"):
+        lat.clover_la_logdet(2.0, m)
+
+
+def test_hmc_clover_logdet_trajectory_matches_oracle_trajectory():
+    """Nf=2 standard clover fermions with the log-det terms in the action and
+    the force (WITH_CLOVER_EO: mon_hmc.c:60-67, force_hmc.c:185-190), SU(3)
+    fundamental, csw=1.2: dH and the final links against the oracle-driven one."""
+    from hirep_b200.hmc import HMC
+
+    dims, ng, beta, mass, csw = (4, 4, 4, 4), 3, 5.6, -0.3, 1.2
+    o = O.Oracle(*dims, ng, O.FUND)
+    u0 = F.smooth_gauge(97, o.V, ng, 0.2)
+    lat = G.Lattice(*dims, ng, G.FUND, ipt=o.geometry()[0])
+    lat.set_gauge(u0)
+    lat.represent_gauge_field(True)
+    lat.clover_init(csw)
+    hmc = HMC(lat, beta, mass, tau=0.5, nsteps=8, force_err2=1e-26, mt_err2=1e-28, force_solver="cg")
+    res = hmc.trajectory(np.random.default_rng(16), metropolis=False)
+    dH_o, u_o = _oracle_trajectory(o, u0, beta, mass, 0.5, 8, np.random.default_rng(16), 1e-26, 1e-28,
+                                   clover_csw=csw)
+    assert abs(res["dH"] - dH_o) < 1e-8 * max(1.0, abs(dH_o)), (res["dH"], dH_o)
+    assert np.abs(lat.gauge_get() - u_o).max() < 1e-10
+
+
 @pytest.mark.parametrize("solver", ["cg_mixed", "g5qmr"])
 def test_hmc_force_solver_forms_agree(solver):
     from hirep_b200.hmc import HMC

@@ -451,3 +451,42 @@ def test_expclover_hmc_energy_violation_scales_as_dt_squared():
         dh[n], _ = oracle_trajectory(o, u0, 5.6, -0.3, 0.5, n, np.random.default_rng(15), 1e-26, 1e-28,
                                      expclover_csw=1.2)
     assert 3.5 < dh[8] / dh[16] < 4.5, dh
+
+
+def test_clover_logdet_hmc_energy_violation_scales_as_dt_squared():
+    """An oracle HMC trajectory with Nf=2 standard clover fermions, log-det terms
+    included (clover_la_logdet in the action, force_clover_logdet in the force):
+    dH falls as dt^2, so the log-det force is the derivative of the log-det action."""
+    from hmc_oracle import oracle_trajectory
+    from hirep_b200 import fields as F
+
+    dh = {}
+    for n in (8, 16):
+        o = O.Oracle(4, 4, 4, 4, 3, O.FUND)
+        u0 = F.smooth_gauge(97, o.V, 3, 0.2)
+        dh[n], _ = oracle_trajectory(o, u0, 5.6, -0.3, 0.5, n, np.random.default_rng(16), 1e-26, 1e-28,
+                                     clover_csw=1.2)
+    assert 3.5 < dh[8] / dh[16] < 4.5, dh
+
+
+def test_clover_la_logdet_is_log_det_of_the_odd_diagonal():
+    """clover_la_logdet subtracts nf log det((4+m) + A) on every odd site
+    (clover_tools.c:312-331), the determinant of the dense 2NF x 2NF blocks."""
+    o = O.Oracle(4, 4, 4, 4, 2, O.FUND)
+    from hirep_b200 import fields as F
+
+    o.set_gauge(o.represent_gauge_field(F.smooth_gauge(3, o.V, 2, 0.4), True))
+    o.clover_init(1.3)
+    o.compute_clover_term()
+    m = -0.4
+    la = o.clover_la_logdet(2.0, m, np.zeros(o.V))
+    assert np.all(la[: o.VH] == 0.0)
+    cl = o.clover_term().reshape(o.V, 4, o.nf, o.nf)
+    nf = o.nf
+    for ix in (o.VH, o.VH + 7, o.V - 1):
+        det = 1.0
+        for b in range(2):
+            s0, s1 = cl[ix, 2 * b], cl[ix, 2 * b + 1]
+            blk = np.block([[s0, s1], [s1.conj().T, -s0]]) + (4 + m) * np.eye(2 * nf)
+            det *= np.linalg.det(blk).real
+        assert abs(la[ix] + 2.0 * np.log(det)) < 1e-12 * abs(la[ix])
