@@ -499,7 +499,9 @@ H_DIMS, H_NG, H_BETA, H_MASS, H_EPS, H_SEED = (64, 32, 32, 32), 2, 2.25, -1.0, 0
 
 def run_hmc_check(torch, G, F):
     """One trajectory with mixed-precision force solves against the same trajectory
-    (same random numbers) with plain FP64 force solves."""
+    (same random numbers) with plain FP64 force solves.  Each form first runs an
+    untimed 2-step warm-up trajectory (kernel autotuning, CUDA-graph capture,
+    work buffers), as every other timed leg has warm-up steps."""
     from hirep_b200.hmc import HMC
 
     lat = G.Lattice(*H_DIMS, H_NG, G.ADJ)
@@ -507,6 +509,10 @@ def run_hmc_check(torch, G, F):
     out = {"workload": "SU(2) adjoint Nf=2 Wilson m0=-1.0 + plaquette beta=2.25, 32^3x64, U=exp(i0.2H) seed 99; "
                        "O2MN tau=1, 20 steps; force solves 1e-10, accept/reject 1e-14"}
     for name, solver in (("mixed", "cg_mixed"), ("fp64", "cg")):
+        lat.set_gauge(u0)
+        lat.represent_gauge_field(True)
+        HMC(lat, H_BETA, H_MASS, tau=0.1, nsteps=2, force_err2=1e-20, mt_err2=1e-28,
+            force_solver=solver).trajectory(np.random.default_rng(H_SEED + 1), metropolis=False)
         lat.set_gauge(u0)
         lat.represent_gauge_field(True)
         plaq0 = lat.avr_plaquette()

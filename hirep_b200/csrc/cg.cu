@@ -238,7 +238,7 @@ struct CGGraph {
   int op = -1;
   double mass = 0;
   const void *ptrs[10] = {};
-  int v[3] = {-1, -1, -1}, force = -1, flt_links = -1;
+  int v[3] = {-1, -1, -1}, force = -1, flt_links = -1, pdl = -1;
   unsigned long mvm = 0;  // hop launches in one replay (the MVM counter)
   cudaGraphExec_t exec = nullptr;
 };
@@ -320,7 +320,8 @@ static int cg_chunk(int op, int prec, double mass, CGWork &w, void *k, void *r, 
   const void *ptrs[10] = {k, r, Mk, w.S, w.d_ptrs, L.partials, links, L.cur_stop,
                           prec == HRGPU_DOUBLE ? L.tmp_e : L.tmp_e_f, prec == HRGPU_DOUBLE ? L.tmp_o : L.tmp_o_f};
   CGGraph &c = CGG[prec];
-  bool same = c.exec && c.op == op && c.mass == mass && c.force == L.hop_force && c.flt_links == L.flt_links;
+  bool same = c.exec && c.op == op && c.mass == mass && c.force == L.hop_force && c.flt_links == L.flt_links &&
+              c.pdl == (int)L.hop_pdl;
   for (int i = 0; i < 3 && same; i++) same = c.v[i] == L.hop_variant[pi][i];
   for (int i = 0; i < 10 && same; i++) same = c.ptrs[i] == ptrs[i];
   if (!same) {
@@ -351,6 +352,7 @@ static int cg_chunk(int op, int prec, double mass, CGWork &w, void *k, void *r, 
     c.mass = mass;
     c.force = L.hop_force;
     c.flt_links = L.flt_links;
+    c.pdl = (int)L.hop_pdl;
     for (int i = 0; i < 3; i++) c.v[i] = L.hop_variant[pi][i];
     for (int i = 0; i < 10; i++) c.ptrs[i] = ptrs[i];
     c.mvm = dm;

@@ -272,6 +272,11 @@ int hrgpu_hop_tuning(int prec, int epilogue, int *chosen, float *ms) {
   return 0;
 }
 
+int hrgpu_set_hop_pdl(int on) {
+  L.hop_pdl = on != 0;
+  return 0;
+}
+
 unsigned long hrgpu_getMVM(void) {
   unsigned long r = g_mvm >> 1;
   g_mvm = 0;

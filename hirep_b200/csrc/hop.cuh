@@ -349,8 +349,19 @@ __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb) {
   return nrm;
 }
 
+// Programmatic dependent launch: let the next kernel of the stream be scheduled
+// as soon as every block of this one has started (its blocks then fill the SMs
+// that this launch's last, partial wave leaves idle), and wait for the previous
+// kernel and its memory before touching global memory.  Both are no-ops for a
+// launch without the programmatic-serialization attribute.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 template <int NFT, bool REAL, typename R, int EP, int MINB, typename LE = typename LinkE<REAL, R>::T>
 __global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop(HopArgs<R> a) {
+  pdl_enter();
   if (a.stop && *a.stop) return;
   const int cb = a.cb0 + blockIdx.x * blockDim.x + threadIdx.x;
   double nrm = 0.0;
@@ -517,6 +528,7 @@ __device__ __forceinline__ double hop2_site(const HopArgs<R> &a, const int cb, c
 
 template <int NFT, bool REAL, typename R, int EP, int MINB, typename LE = typename LinkE<REAL, R>::T>
 __global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop2(HopArgs<R> a) {
+  pdl_enter();
   if (a.stop && *a.stop) return;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = a.cb0 + (tid >> 1) < a.cb1;

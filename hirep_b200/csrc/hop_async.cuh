@@ -61,6 +61,7 @@ __global__ void __launch_bounds__(HOP_THREADS) k_hop_async(HopArgs<R> a) {
   const int nf = NFT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const Geo g = a.g;
+  pdl_enter();
   if (a.stop && *a.stop) return;
   const int tid = threadIdx.x;
   const int cs = a.cb0 + blockIdx.x * blockDim.x + tid;

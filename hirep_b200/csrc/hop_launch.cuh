@@ -7,6 +7,30 @@
 
 namespace hrgpu {
 
+// A whole-lattice FP64 hop is launched with programmatic stream serialisation
+// (the kernels wait on their predecessor with griddepcontrol.wait before
+// reading memory), so its blocks fill the SMs the previous hop's last wave
+// leaves idle: Cphi_eopre 62.5 -> 60.4 us at 16^3x32 (alternating A/B in one
+// process), the FP64 CG unchanged.  Without it: FP32 hops (inside the mixed
+// solve's graphs it cost 3 %: 18.7 -> 19.3 ms) and launches over a few time
+// slabs (the host-field pipeline, where the early, waiting blocks held SMs
+// that the copy-stream kernels beside them needed: 0.47 -> 0.69 ms).
+template <typename R>
+static inline cudaError_t launch_pdl(void (*kernel)(HopArgs<R>), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                     HopArgs<R> &a) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = (L.hop_pdl && sizeof(R) == 8 && a.cb0 == 0 && a.cb1 == (int)L.VH) ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, a);
+}
+
 template <int N, bool RL, typename R, int EP>
 int launch_async(HopArgs<R> &a, dim3 grid, dim3 block, cudaStream_t s) {
   if constexpr (AsyncOK<N, RL>::v) {
@@ -16,7 +40,7 @@ int launch_async(HopArgs<R> &a, dim3 grid, dim3 block, cudaStream_t s) {
       HR_CUDA(cudaFuncSetAttribute(k_hop_async<N, RL, R, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
       attr = true;
     }
-    k_hop_async<N, RL, R, EP><<<grid, block, smem, s>>>(a);
+    HR_CUDA(launch_pdl<R>(k_hop_async<N, RL, R, EP>, grid, block, smem, s, a));
     return 0;
   } else {
     return -1;  // not built for this NF
@@ -37,10 +61,10 @@ int launch_ep_variant(HopArgs<R> &a, int variant) {
 #define HOPV(N, RL)                                                                    \
   case N:                                                                              \
     switch (variant) {                                                                 \
-      case 0: k_hop<N, RL, R, EP, 1><<<grid, block, 0, s>>>(a); break;                 \
-      case 1: k_hop2<N, RL, R, EP, 1><<<grid, block, 0, s>>>(a); break;                \
-      case 2: k_hop<N, RL, R, EP, 4><<<grid, block, 0, s>>>(a); break;                 \
-      case 3: k_hop2<N, RL, R, EP, 4><<<grid, block, 0, s>>>(a); break;                \
+      case 0: HR_CUDA(launch_pdl<R>(k_hop<N, RL, R, EP, 1>, grid, block, 0, s, a)); break;  \
+      case 1: HR_CUDA(launch_pdl<R>(k_hop2<N, RL, R, EP, 1>, grid, block, 0, s, a)); break; \
+      case 2: HR_CUDA(launch_pdl<R>(k_hop<N, RL, R, EP, 4>, grid, block, 0, s, a)); break;  \
+      case 3: HR_CUDA(launch_pdl<R>(k_hop2<N, RL, R, EP, 4>, grid, block, 0, s, a)); break; \
       default:                                                                         \
         if (int rc_ = launch_async<N, RL, R, EP>(a, grid, block, s)) return rc_;       \
         break;                                                                         \
@@ -52,10 +76,10 @@ int launch_ep_variant(HopArgs<R> &a, int variant) {
 #define HOPVB(N, RL)                                                                            \
   case N:                                                                                       \
     switch (variant) {                                                                          \
-      case 0: k_hop<N, RL, float, EP, 1, typename LinkBF16<RL>::T><<<grid, block, 0, s>>>(a); break;  \
-      case 1: k_hop2<N, RL, float, EP, 1, typename LinkBF16<RL>::T><<<grid, block, 0, s>>>(a); break; \
-      case 2: k_hop<N, RL, float, EP, 4, typename LinkBF16<RL>::T><<<grid, block, 0, s>>>(a); break;  \
-      case 3: k_hop2<N, RL, float, EP, 4, typename LinkBF16<RL>::T><<<grid, block, 0, s>>>(a); break; \
+      case 0: HR_CUDA(launch_pdl<float>(k_hop<N, RL, float, EP, 1, typename LinkBF16<RL>::T>, grid, block, 0, s, a)); break;  \
+      case 1: HR_CUDA(launch_pdl<float>(k_hop2<N, RL, float, EP, 1, typename LinkBF16<RL>::T>, grid, block, 0, s, a)); break; \
+      case 2: HR_CUDA(launch_pdl<float>(k_hop<N, RL, float, EP, 4, typename LinkBF16<RL>::T>, grid, block, 0, s, a)); break;  \
+      case 3: HR_CUDA(launch_pdl<float>(k_hop2<N, RL, float, EP, 4, typename LinkBF16<RL>::T>, grid, block, 0, s, a)); break; \
       default: return -1;                                                                       \
     }                                                                                           \
     break;

@@ -102,6 +102,7 @@ struct Lattice {
   // tuned hopping-kernel variant [FP64, FP32, FP32 with BF16 links][epilogue]
   int hop_variant[3][3] = {{-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}};
   int hop_force = -1;             // forced variant (-1: autotune)
+  bool hop_pdl = true;            // whole-lattice hops with programmatic dependent launch
   float hop_tune_ms[3][3][HOP_VARIANTS] = {};  // tuning times of the variants [slot][epilogue][variant]
   // storage of the links read by the FP32 operators: HRGPU_LINKS_F32 (Uf) or HRGPU_LINKS_BF16 (Ubf)
   int flt_links = 0;

@@ -143,6 +143,10 @@ int hrgpu_g5Dphi_eopre_sq_flt(double m0, void *out, const void *in);
  * measured (ms has room for 5 values; -1 marks a variant not built for this NF);
  * precision 2 is the FP32 operator reading BF16 links.
  * Tuning controls of this library; they have no counterpart in the reference. */
+/* whole-lattice FP64 hopping kernels launched with programmatic dependent
+ * launch (default 1: the next hop's blocks start in the SMs the previous hop's
+ * last wave leaves idle); 0 launches them plainly */
+int hrgpu_set_hop_pdl(int on);
 int hrgpu_set_hop_variant(int variant);
 int hrgpu_hop_tuning(int prec, int epilogue, int *chosen, float *ms);
 /* Storage of the links read by the FP32 operators (the _flt operators, the

@@ -319,3 +319,25 @@ def test_hop_variants(variant, ng, rep):
         assert rel(out32.download(), o.g5Dphi_eopre_flt(m, e32)) < 10 * TOL32
     finally:
         G._check(lat.L.hrgpu_set_hop_variant(-1), "set_hop_variant")
+
+
+def test_programmatic_dependent_launch_changes_no_result():
+    """FP64 hops with and without programmatic dependent launch: the same
+    kernels, so bit-identical operators and solves."""
+    o, lat, _, _ = setup((4, 4, 4, 4), 3, O.FUND, seed=31, smooth=0.3)
+    lat.clover_init(1.0)
+    m = -0.2
+    e = F.gaussian_spinor(8, o.VH, o.nf)
+    fin, fout = lat.field(O.EVEN, host=e), lat.field(O.EVEN)
+    res = {}
+    try:
+        for pdl in (1, 0):
+            G._check(lat.L.hrgpu_set_hop_pdl(pdl), "set_hop_pdl")
+            lat.g5Cphi_eopre_sq(m, fout, fin)
+            x = lat.field(O.EVEN)
+            lat.cg_mshift(G.OP_G5CPHI_EOPRE_SQ, m, [0.0], 1e-24, fin, [x])
+            res[pdl] = (fout.download(), x.download())
+    finally:
+        G._check(lat.L.hrgpu_set_hop_pdl(1), "set_hop_pdl")
+    assert np.array_equal(res[0][0], res[1][0])
+    assert np.array_equal(res[0][1], res[1][1])
