@@ -24,10 +24,11 @@
 // replayed: its chunks cost tens of API calls that the host would otherwise
 // issue while the copies run.  (Kernels that read and write the mapped host
 // buffers directly were measured too: their PCIe traffic slowed the hops
-// running beside them and the pipeline was no faster.)  The graph is cached per (operator, precision,
-// mass, host buffers, chunking, kernel variants, link storage); the data it
-// reads (links, clover blocks) are read at replay, so new gauge fields need
-// no new graph.  Pageable buffers take the eager path.
+// running beside them and the pipeline was no faster.)  The graph is cached
+// per (operator, precision, mass, host buffers, chunking, kernel variants,
+// launch mode, link storage); the data it reads (links, clover blocks) are
+// read at replay, so new gauge fields need no new graph.  Pageable buffers
+// take the eager path.
 //
 // The device layout puts the time coordinate slowest, so a time slab of one
 // parity is one contiguous range of checkerboard indices, [t S, (t+1) S) with
@@ -61,7 +62,7 @@ struct HostGraph {
   const void *hin;
   void *hout;
   const void *U;
-  int v0, v1, flt_links;
+  int v0, v1, flt_links, pdl;
   long VH;
   cudaGraphExec_t exec = nullptr;
 };
@@ -284,12 +285,13 @@ static int apply_host(int clover, int g5, double mass, void *host_out, const voi
     key.v0 = L.hop_force >= 0 ? 100 + L.hop_force : L.hop_variant[pi][e0];
     key.v1 = L.hop_force >= 0 ? 100 + L.hop_force : L.hop_variant[pi][e1];
     key.flt_links = L.flt_links;
+    key.pdl = (int)L.hop_pdl;
     key.VH = L.VH;
     HostGraph *hit = nullptr;
     for (HostGraph &h : HG)
       if (h.clover == key.clover && h.g5 == key.g5 && h.prec == key.prec && h.K == key.K && h.mass == key.mass &&
           h.hin == key.hin && h.hout == key.hout && h.U == key.U && h.v0 == key.v0 && h.v1 == key.v1 &&
-          h.flt_links == key.flt_links && h.VH == key.VH)
+          h.flt_links == key.flt_links && h.pdl == key.pdl && h.VH == key.VH)
         hit = &h;
     if (!hit) {
       if (HG.size() >= HG_MAX) free_graphs();
