@@ -2,16 +2,21 @@
 
 update_ghmc (LibHR/Update/update_mt.c:148-260) with two monomials: the
 plaquette gauge action (mon_pg.c; force0.c) and an Nf = 2 Wilson pseudofermion
-on the even sites (mon_hmc.c; force_hmc.c, UPDATE_EO branch), integrated with
-the second-order Omelyan integrator (integrators.c:64-93, lambda =
-0.1931833275037836).  With a clover term the fermion operator is Cphi_eopre
+on the even sites (mon_hmc.c; force_hmc.c, UPDATE_EO branch).  The integrator
+is HiRep's multilevel scheme (integrators.c): a list of levels, each with an
+integrator (leapfrog, O2MN or O4MN), a number of steps and the monomials whose
+forces it applies; a level's field update moves the links if the gauge
+monomial (which owns update_gauge_field, mon_pg.c:71) sits on it and then runs
+the next level for the same time.  The default is one O2MN level with both
+monomials.  With a clover term the fermion operator is Cphi_eopre
 (D_update.c:26-95) and the clover force is part of force_fermion_core.  The
 standard clover monomial also carries the log-det terms of WITH_CLOVER_EO:
 clover_la_logdet(2, m) in its local action (mon_hmc.c:60-67) and
 force_clover_logdet(m, 2) in its force (force_hmc.c:185-190, logdet = 1 as
 mon_hmc.c:109 sets it); the exponential clover term (WITH_EXPCLOVER) has none
-(its blocks are traceless, det D_oo is constant).  Links, momenta and pseudofermions stay on the device; the
-host only holds the scalars of the recursion and the random numbers.
+(its blocks are traceless, det D_oo is constant).  Links, momenta and
+pseudofermions stay on the device; the host only holds the scalars of the
+recursion and the random numbers.
 
 The force solves are either HiRep's (two g5QMR solves on D) or, as the
 mixed-precision form of this library, one CG on H^2 = (g5 D)^2 (FP64 or FP32
@@ -25,13 +30,66 @@ import numpy as np
 from . import hrgpu as G
 
 LAMBDA_O2MN = 0.1931833275037836
+# fourth-order Omelyan-Mryglod-Folk (Comput. Phys. Commun. 151 (2003) 272), in
+# the form of Takaishi and de Forcrand (hep-lat/0505020) that integrators.c uses
+O4MN_RHO, O4MN_THETA, O4MN_LAMBDA = 0.1786178958448091, -0.06626458266981843, 0.7123418310626056
+INTEGRATORS = ("leapfrog", "o2mn", "o4mn")
+MONOMIALS = ("gauge", "fermion")
+
+
+def integrate(kind, nsteps, tlen, force, field):
+    """One level of the multilevel integrator (integrators.c:30-132):
+    force(dt) kicks the momenta with the level's monomials, field(dt) moves
+    the links and runs the next level."""
+    if nsteps == 0:
+        return
+    dt = tlen / nsteps
+    if kind == "leapfrog":  # leapfrog_multistep
+        for n in range(nsteps):
+            force(dt / 2 if n == 0 else dt)
+            field(dt)
+        force(dt / 2)
+    elif kind == "o2mn":  # O2MN_multistep
+        lam = LAMBDA_O2MN
+        for n in range(nsteps):
+            force(lam * dt if n == 0 else 2 * lam * dt)
+            field(dt / 2)
+            force((1 - 2 * lam) * dt)
+            field(dt / 2)
+        force(lam * dt)
+    elif kind == "o4mn":  # O4MN_multistep
+        rho, theta, lam = O4MN_RHO, O4MN_THETA, O4MN_LAMBDA
+        for n in range(nsteps):
+            force(rho * dt if n == 0 else 2 * rho * dt)
+            field(lam * dt)
+            force(theta * dt)
+            field((0.5 - lam) * dt)
+            force((1 - 2 * (theta + rho)) * dt)
+            field((0.5 - lam) * dt)
+            force(theta * dt)
+            field(lam * dt)
+        force(rho * dt)
+    else:
+        raise ValueError(f"integrator {kind!r}: one of {INTEGRATORS}")
 
 
 class HMC:
     def __init__(self, lat, beta, mass, tau, nsteps, force_err2=1e-20, mt_err2=1e-28, force_solver="cg_mixed",
-                 bc_t_antiperiodic=True):
+                 bc_t_antiperiodic=True, levels=None):
+        """levels: [(integrator, nsteps, monomials), ...] from the outermost level
+        in; None is [("o2mn", nsteps, ("gauge", "fermion"))]."""
         if force_solver not in ("cg_mixed", "cg", "g5qmr"):
             raise ValueError("force_solver: cg_mixed, cg or g5qmr")
+        if levels is None:
+            levels = [("o2mn", nsteps, MONOMIALS)]
+        seen = []
+        for kind, n, mons in levels:
+            if kind not in INTEGRATORS or n < 0 or any(m not in MONOMIALS for m in mons):
+                raise ValueError(f"bad integrator level {(kind, n, mons)}")
+            seen += list(mons)
+        if sorted(seen) != sorted(MONOMIALS):
+            raise ValueError("each monomial (gauge, fermion) must sit on exactly one level")
+        self.levels = [(kind, n, tuple(mons)) for kind, n, mons in levels]
         self.lat, self.beta, self.mass, self.tau, self.nsteps = lat, beta, mass, tau, nsteps
         self.force_err2, self.mt_err2, self.force_solver = force_err2, mt_err2, force_solver
         self.bc = bc_t_antiperiodic
@@ -86,25 +144,29 @@ class HMC:
         lat.fermion_force_end_momenta(dt)
         self.nforce += 1
 
-    def force(self, dt):
-        """monomial_force (integrators.c:12-19): every monomial's force."""
-        self.lat.force0(dt, self.beta)
-        self.fermion_force(dt)
+    def force(self, level, dt):
+        """monomial_force (integrators.c:12-19): the forces of the level's monomials."""
+        for m in self.levels[level][2]:
+            if m == "gauge":
+                self.lat.force0(dt, self.beta)
+            else:
+                self.fermion_force(dt)
 
-    def field(self, dt):
-        """monomial_field: the gauge monomial's update_gauge_field."""
-        self.lat.update_gauge_field(dt)
+    def field(self, level, dt):
+        """monomial_field (integrators.c:21-33): update_gauge_field if the gauge
+        monomial is on this level, then the next level for the same time."""
+        if "gauge" in self.levels[level][2]:
+            self.lat.update_gauge_field(dt)
+        if level + 1 < len(self.levels):
+            self.run_level(level + 1, dt)
 
-    def o2mn(self):
-        """O2MN_multistep (integrators.c:64-93)."""
-        dt = self.tau / self.nsteps
-        lam = LAMBDA_O2MN
-        for n in range(self.nsteps):
-            self.force(lam * dt if n == 0 else 2 * lam * dt)
-            self.field(dt / 2)
-            self.force((1 - 2 * lam) * dt)
-            self.field(dt / 2)
-        self.force(lam * dt)
+    def run_level(self, level, tlen):
+        kind, n, _ = self.levels[level]
+        integrate(kind, n, tlen, lambda dt: self.force(level, dt), lambda dt: self.field(level, dt))
+
+    def md(self):
+        """The molecular dynamics evolution of one trajectory (tau)."""
+        self.run_level(0, self.tau)
 
     # -- one trajectory -------------------------------------------------------------
     def trajectory(self, rng, metropolis=True):
@@ -126,7 +188,7 @@ class HMC:
         lat.la("zero", self.y)
         self.iters = 0
         self.nforce = 0
-        self.o2mn()
+        self.md()
         lat.project_gauge_field()
         lat.represent_gauge_field(self.bc)
         # correct_la_pf: pf <- H^-1 pf = D^-1 g5 pf (g5QMR, FP64, MT precision)

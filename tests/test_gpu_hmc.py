@@ -172,6 +172,61 @@ def test_hmc_clover_logdet_trajectory_matches_oracle_trajectory():
     assert np.abs(lat.gauge_get() - u_o).max() < 1e-10
 
 
+def test_hmc_nested_o4mn_trajectory_matches_oracle_trajectory():
+    """Two integrator levels as HiRep nests them (integrators.c:21-33): O4MN with
+    the fermion monomial outside, O4MN with the gauge monomial (and the link
+    updates) inside; clover with log-det terms.  dH and the final links against
+    the oracle-driven trajectory."""
+    from hirep_b200.hmc import HMC
+
+    dims, ng, beta, mass, csw = (4, 4, 4, 4), 2, 6.0, -0.8, 1.0
+    levels = [("o4mn", 3, ("fermion",)), ("o4mn", 4, ("gauge",))]
+    o = O.Oracle(*dims, ng, O.ADJ)
+    u0 = F.smooth_gauge(41, o.V, ng, 0.3)
+    lat = G.Lattice(*dims, ng, G.ADJ, ipt=o.geometry()[0])
+    lat.set_gauge(u0)
+    lat.represent_gauge_field(True)
+    lat.clover_init(csw)
+    hmc = HMC(lat, beta, mass, tau=0.2, nsteps=0, force_err2=1e-26, mt_err2=1e-28, force_solver="cg", levels=levels)
+    res = hmc.trajectory(np.random.default_rng(17), metropolis=False)
+    dH_o, u_o = _oracle_trajectory(o, u0, beta, mass, 0.2, 0, np.random.default_rng(17), 1e-26, 1e-28,
+                                   clover_csw=csw, levels=levels)
+    assert abs(res["dH"] - dH_o) < 1e-8 * max(1.0, abs(dH_o)), (res["dH"], dH_o)
+    assert np.abs(lat.gauge_get() - u_o).max() < 1e-10
+    assert res["force_evaluations"] == 4 * 3 + 1  # O4MN: four fermion kicks a step and a last one
+
+
+def test_md_reversibility():
+    """TestProgram/Update/check_update_1 restated: from a random (hot) start on
+    8x4^3 (SU(2) adjoint, clover csw=1.0 with log-det terms, m0=-0.8, beta=6.0),
+    tau=0.2 with O4MN/O4MN nested 10/10, then the momenta flipped and the same
+    evolution again: the plaquette returns to 1e-10 (the reference's bound)."""
+    from hirep_b200.hmc import HMC
+
+    dims, ng = (8, 4, 4, 4), 2
+    lat = G.Lattice(*dims, ng, G.ADJ)
+    lat.set_gauge(F.hot_gauge(35563, lat.V, ng))
+    lat.represent_gauge_field(True)
+    lat.clover_init(1.0)
+    hmc = HMC(lat, 6.0, -0.8, tau=0.2, nsteps=0, force_err2=1e-26, force_solver="cg",
+              levels=[("o4mn", 10, ("fermion",)), ("o4mn", 10, ("gauge",))])
+    rng = np.random.default_rng(3)
+    lat.set_dirac_mass(-0.8)
+    u0, plaq0 = lat.gauge_get(), lat.avr_plaquette()
+    lat.momenta_set(rng.standard_normal((lat.V, 4, lat.dimg)) / np.sqrt(0.5))
+    eta = lat.field(G.EVEN, host=(rng.standard_normal((lat.VH, 4, lat.nf))
+                                  + 1j * rng.standard_normal((lat.VH, 4, lat.nf))) / np.sqrt(2))
+    hmc.apply_h(-0.8, hmc.pf, eta)
+    lat.la("zero", hmc.y)
+    hmc.md()
+    plaq1 = lat.avr_plaquette()
+    lat.momenta_set(-lat.momenta_get())  # flip_mom (update_mt.c:310)
+    hmc.md()
+    assert abs(plaq1 - plaq0) > 1e-3  # the evolution moved the links
+    assert abs(lat.avr_plaquette() - plaq0) < 1e-10
+    assert np.abs(lat.gauge_get() - u0).max() < 1e-8
+
+
 @pytest.mark.parametrize("solver", ["cg_mixed", "g5qmr"])
 def test_hmc_force_solver_forms_agree(solver):
     from hirep_b200.hmc import HMC

@@ -490,3 +490,20 @@ def test_clover_la_logdet_is_log_det_of_the_odd_diagonal():
             blk = np.block([[s0, s1], [s1.conj().T, -s0]]) + (4 + m) * np.eye(2 * nf)
             det *= np.linalg.det(blk).real
         assert abs(la[ix] + 2.0 * np.log(det)) < 1e-12 * abs(la[ix])
+
+
+@pytest.mark.parametrize("kind,ratio", [("o4mn", (14.0, 19.0)), ("leapfrog", (3.5, 4.5))])
+def test_integrator_orders(kind, ratio):
+    """Oracle trajectories with HiRep's O4MN (integrators.c:95-132) and leapfrog
+    (:30-52) integrators: halving dt divides dH by 2^4 (measured 16.6 from 8 to
+    16 steps) and by 2^2 (4.1), which pins their coefficients."""
+    from hmc_oracle import oracle_trajectory
+    from hirep_b200 import fields as F
+
+    dh = {}
+    for n in (8, 16):
+        o = O.Oracle(4, 4, 4, 4, 2, O.ADJ)
+        u0 = F.smooth_gauge(7, o.V, 2, 0.3)
+        dh[n], _ = oracle_trajectory(o, u0, 2.25, -1.0, 0.5, n, np.random.default_rng(8), 1e-28, 1e-28,
+                                     levels=[(kind, n, ("gauge", "fermion"))])
+    assert ratio[0] < dh[8] / dh[16] < ratio[1], dh
