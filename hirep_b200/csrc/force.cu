@@ -520,6 +520,14 @@ int hrgpu_fermion_force_end(double dt, double *force_host) {
   return rc;
 }
 
+// cl_force (the six sigma-insertion matrices per site that force_fermion_core's
+// clover part accumulates) in HiRep's layout [V][6][NF*NF] complex
+int hrgpu_clover_force_get(void *host) {
+  HR_REQUIRE(L.ready && L.clover && L.cl_force, HRGPU_E_STATE, "clover_force_get: no clover force accumulated");
+  HR_REQUIRE(host, HRGPU_E_ARG, "clover_force_get: NULL output");
+  return links_out(host, L.cl_force, L.nf * L.nf, 16, 6);
+}
+
 int hrgpu_force_sum_get(double *host) {
   HR_REQUIRE(L.ready && L.force_sum, HRGPU_E_STATE, "force_sum_get: no force accumulated");
   return links_out(host, L.force_sum, L.dimg, 8, 4);

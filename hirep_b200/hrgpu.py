@@ -244,6 +244,11 @@ class Lattice:
         _check(self.L.hrgpu_clover_term_get(_ptr(cl)), "clover_term_get")
         return cl
 
+    def clover_force(self):
+        cf = np.empty((self.V, 6, self.nf, self.nf), np.complex128)
+        _check(self.L.hrgpu_clover_force_get(_ptr(cf)), "clover_force_get")
+        return cf
+
     def Cphi(self, m, out, inp): self._m("Cphi", m, out, inp)
     def g5Cphi(self, m, out, inp): self._m("g5Cphi", m, out, inp)
     def g5Cphi_sq(self, m, out, inp): self._m("g5Cphi_sq", m, out, inp)

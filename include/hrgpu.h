@@ -380,6 +380,7 @@ int hrgpu_force_clover_logdet(double mass, double residue); /* force_fermion_cor
 /* fermion_force_end (force_fermion_core.c:964-993): clover derivative, then adds the
  * accumulated force to the host momentum field force[V][4][NG*NG-1] (HiRep layout) */
 int hrgpu_fermion_force_end(double dt, double *force_host);
+int hrgpu_clover_force_get(void *host); /* cl_force in HiRep layout [V][6][NF*NF] complex */
 /* the accumulator itself, HiRep layout (for tests) */
 int hrgpu_force_sum_get(double *host);
 

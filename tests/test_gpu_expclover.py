@@ -109,3 +109,28 @@ def test_expclover_force_matches_oracle(ng, rep):
     fo = o.fermion_force_end(0.7, mom.copy())
     fg = lat.fermion_force_end(0.7, mom.copy())
     assert rel(fg, fo) < 1e-12
+
+
+@pytest.mark.parametrize("ng", [2, 3])
+def test_expclover_force_matrices_two_forms(ng):
+    """TestProgram/Update/check_update_2 restated: the exponential clover force
+    matrices cl_force from Z2 volume sources, computed two ways - the oracle's
+    Taylor form (force_clover_fermion_taylor) and the device's Frechet
+    derivative by scaling and squaring - agree to an RMS of 1e-14 per element
+    (the reference's bound), SU(2) and SU(3) fundamental as there."""
+    o, lat = setup(ng, O.FUND, seed=23)
+    m = -0.5
+    o.set_mass(m)
+    lat.set_dirac_mass(m)
+    rng = np.random.default_rng(ng)
+
+    def z2():
+        return ((rng.integers(0, 2, (o.V, 4, o.nf)) * 2 - 1) + 1j * (rng.integers(0, 2, (o.V, 4, o.nf)) * 2 - 1)) / np.sqrt(2)
+
+    X, Y = z2(), z2()
+    o.fermion_force_begin()
+    o.force_fermion_core(X, Y, 0, 1.0, 1.0)
+    lat.fermion_force_begin()
+    lat.force_fermion_core(lat.field(O.FULL, host=X), lat.field(O.FULL, host=Y), 0, 1.0, 1.0)
+    d = lat.clover_force() - o.clover_force().reshape(o.V, 6, o.nf, o.nf)
+    assert np.sqrt(np.sum(np.abs(d) ** 2) / (o.V * 6 * o.nf * o.nf)) < 1e-14
