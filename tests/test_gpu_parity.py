@@ -341,3 +341,59 @@ def test_programmatic_dependent_launch_changes_no_result():
         G._check(lat.L.hrgpu_set_hop_pdl(1), "set_hop_pdl")
     assert np.array_equal(res[0][0], res[1][0])
     assert np.array_equal(res[0][1], res[1][1])
+
+
+def test_spin_structure_gamma_matrices():
+    """TestProgram/DiracOperator/check_diracoperator_4 restated: with every link
+    zero but U(g, mu) = 1 (periodic BCs) and a constant source in spin beta,
+    colour ic, Dphi_ gives out(g) - out(g+mu) = gamma_mu column beta.  The
+    extracted gammas are the same for every site and colour (1e-14, as the
+    reference requires), Hermitian, satisfy {g_mu, g_nu} = 2 delta, and
+    diag(1,1,-1,-1) (the gamma_5 of g5Dphi) anticommutes with them and equals
+    +-g0 g1 g2 g3."""
+    dims = (4, 4, 4, 4)
+    T, X, Y, Z = dims
+    ng = 3
+    o = O.Oracle(*dims, ng, O.FUND)
+    ipt = o.geometry()[0]
+    lat = G.Lattice(*dims, ng, G.FUND, ipt=ipt)
+    V, nf = lat.V, lat.nf
+
+    def idx(t, x, y, z):
+        return ipt[((t % T * X + x % X) * Y + y % Y) * Z + z % Z]
+
+    ref = None
+    inp, out = lat.field(O.FULL), lat.field(O.FULL)
+    for g in [(0, 0, 0, 0), (3, 3, 3, 3), (1, 2, 3, 0), (2, 0, 1, 3)]:
+        for ic in (0, nf - 1):
+            gam = np.zeros((4, 4, 4), complex)
+            for mu in range(4):
+                u = np.zeros((V, 4, ng, ng), complex)
+                u[idx(*g), mu] = np.eye(ng)
+                lat.set_gauge(u)
+                lat.represent_gauge_field(False)
+                sh = [0, 0, 0, 0]
+                sh[mu] = 1
+                gp = idx(*(c + s for c, s in zip(g, sh)))
+                for beta in range(4):
+                    src = np.zeros((V, 4, nf), complex)
+                    src[:, beta, ic] = 1.0
+                    inp.upload(src)
+                    lat.Dphi_(out, inp)
+                    r = out.download()
+                    gam[mu, :, beta] = r[idx(*g), :, ic] - r[gp, :, ic]
+                    others = np.ones(V, bool)
+                    others[[idx(*g), gp]] = False
+                    assert np.all(r[others] == 0.0)
+            if ref is None:
+                ref = gam
+            assert np.sum(np.abs(gam - ref) ** 2) < 1e-14
+    eye = np.eye(4)
+    g5 = np.diag([1.0, 1.0, -1.0, -1.0])
+    for mu in range(4):
+        assert np.allclose(ref[mu], ref[mu].conj().T, atol=1e-15)
+        assert np.allclose(g5 @ ref[mu] + ref[mu] @ g5, 0.0, atol=1e-15)
+        for nu in range(4):
+            assert np.allclose(ref[mu] @ ref[nu] + ref[nu] @ ref[mu], 2.0 * eye * (mu == nu), atol=1e-15)
+    prod = ref[0] @ ref[1] @ ref[2] @ ref[3]
+    assert np.allclose(prod, g5, atol=1e-15) or np.allclose(prod, -g5, atol=1e-15)
