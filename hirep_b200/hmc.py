@@ -75,9 +75,12 @@ def integrate(kind, nsteps, tlen, force, field):
 
 class HMC:
     def __init__(self, lat, beta, mass, tau, nsteps, force_err2=1e-20, mt_err2=1e-28, force_solver="cg_mixed",
-                 bc_t_antiperiodic=True, levels=None):
+                 bc_t_antiperiodic=True, levels=None, mre_past=0):
         """levels: [(integrator, nsteps, monomials), ...] from the outermost level
-        in; None is [("o2mn", nsteps, ("gauge", "fermion"))]."""
+        in; None is [("o2mn", nsteps, ("gauge", "fermion"))].  mre_past > 0: the
+        force solves start from the chronological (MRE) guess over that many past
+        solutions (mre.c, as force_hmc.c:122-145 uses it); 0: the g5QMR solves
+        start from zero and the CG solves from the previous solution."""
         if force_solver not in ("cg_mixed", "cg", "g5qmr"):
             raise ValueError("force_solver: cg_mixed, cg or g5qmr")
         if levels is None:
@@ -90,6 +93,7 @@ class HMC:
         if sorted(seen) != sorted(MONOMIALS):
             raise ValueError("each monomial (gauge, fermion) must sit on exactly one level")
         self.levels = [(kind, n, tuple(mons)) for kind, n, mons in levels]
+        self.mre = lat.mre(mre_past, G.EVEN) if mre_past > 0 else None
         self.lat, self.beta, self.mass, self.tau, self.nsteps = lat, beta, mass, tau, nsteps
         self.force_err2, self.mt_err2, self.force_solver = force_err2, mt_err2, force_solver
         self.bc = bc_t_antiperiodic
@@ -121,18 +125,32 @@ class HMC:
         if self.force_solver == "g5qmr":
             # X = H^-1 pf = D^-1 g5 pf, Y = H^-1 X = D^-1 g5 X
             lat.la("g5", self.tmp, self.pf)
-            lat.la("zero", self.x)
+            if self.mre:
+                self.mre.guess(0, self.x, self.op_d, self.mass, self.tmp)
+            else:
+                lat.la("zero", self.x)
             it, ok = lat.g5QMR_mshift(self.op_d, self.mass, [0.0], self.force_err2, self.tmp, [self.x])
+            if self.mre:
+                self.mre.store(0, self.x)
             lat.la("g5", self.tmp, self.x)
-            lat.la("zero", self.y)
+            if self.mre:
+                self.mre.guess(1, self.y, self.op_d, self.mass, self.tmp)
+            else:
+                lat.la("zero", self.y)
             it2, ok2 = lat.g5QMR_mshift(self.op_d, self.mass, [0.0], self.force_err2, self.tmp, [self.y])
+            if self.mre:
+                self.mre.store(1, self.y)
             self.iters += it + it2
             if not (ok and ok2):
                 raise G.HRGPUError("HMC: g5QMR force solve did not converge")
             X, Y = self.x, self.y
         else:
-            # Y = (H^2)^-1 pf (start from the previous solution), X = H Y
+            # Y = (H^2)^-1 pf (start from the MRE guess or the previous solution), X = H Y
+            if self.mre:
+                self.mre.guess(0, self.y, self.op_h2, self.mass, self.pf)
             self._solve(self.op_h2, self.y, self.pf, self.force_err2, self.force_solver == "cg_mixed")
+            if self.mre:
+                self.mre.store(0, self.y)
             self.apply_h(self.mass, self.x, self.y)
             X, Y = self.x, self.y
         self._even_into_full(self.Xs, X)

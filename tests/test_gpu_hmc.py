@@ -227,6 +227,27 @@ def test_md_reversibility():
     assert np.abs(lat.gauge_get() - u0).max() < 1e-8
 
 
+@pytest.mark.parametrize("solver", ["cg", "g5qmr"])
+def test_hmc_mre_guess_changes_no_trajectory(solver):
+    """Force solves started from the MRE chronological guess (mre.c; force_hmc.c:
+    122-145) end at the same trajectory to solver tolerance and take fewer MVMs."""
+    from hirep_b200.hmc import HMC
+
+    dims, ng, beta, mass = (4, 4, 4, 4), 2, 2.25, -1.0
+    u0 = F.smooth_gauge(99, 256, ng, 0.2)
+    out = {}
+    for mre in (0, 3):
+        lat = G.Lattice(*dims, ng, G.ADJ)
+        lat.set_gauge(u0)
+        lat.represent_gauge_field(True)
+        hmc = HMC(lat, beta, mass, tau=0.5, nsteps=10, force_err2=1e-24, force_solver=solver, mre_past=mre)
+        r = hmc.trajectory(np.random.default_rng(6), metropolis=False)
+        out[mre] = (r["dH"], r["force_solve_iters"], lat.gauge_get())
+    assert abs(out[3][0] - out[0][0]) < 1e-7 * max(1.0, abs(out[0][0]))
+    assert np.abs(out[3][2] - out[0][2]).max() < 1e-9
+    assert out[3][1] < out[0][1]
+
+
 @pytest.mark.parametrize("solver", ["cg_mixed", "g5qmr"])
 def test_hmc_force_solver_forms_agree(solver):
     from hirep_b200.hmc import HMC
