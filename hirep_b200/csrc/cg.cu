@@ -47,9 +47,9 @@ __device__ double fold_partials(const double *partials, int nblocks, int stride,
 }
 
 // alpha = <k, Mk>; omega = -delta/alpha; z3 and the solution coefficients (cg_mshift.c:82-91)
-__global__ void k_cg_fold_alpha(CGState *S, const double *partials, int nblocks) {
+__global__ void k_cg_fold_alpha(CGState *S, const double *partials, int nblocks, int stride) {
   if (S->state != 0) return;
-  double alpha = fold_partials(partials, nblocks, 2, 0);
+  double alpha = fold_partials(partials, nblocks, stride, 0);
   if (threadIdx.x == 0) {
     S->alpha = alpha;
     if (!isfinite(alpha) || alpha == 0.0) {  // breakdown (non-positive operator or NaN input)
@@ -286,9 +286,18 @@ static int cg_iterations(int op, int prec, double mass, CGWork &w, void *k, void
   V *const *dx = (V *const *)w.d_ptrs;
   V *const *dp = (V *const *)(w.d_ptrs + MAXS);
   for (int c = 0; c < CG_CHUNK; c++) {
-    if (int rc = apply_op(op, prec, mass, Mk, k)) return rc;
-    k_cg_dot<V><<<g, RED_THREADS, 0, L.stream>>>(w.S, (const V *)k, (const V *)Mk, ne, L.partials);
-    k_cg_fold_alpha<<<1, RED_THREADS, 0, L.stream>>>(w.S, L.partials, g);
+    // alpha = <k, H^2 k> = |H k|^2 from the first H's partials where the
+    // operator is the even-odd H^2, else from a dot-product pass
+    int nb = 0;
+    const int rc = apply_op_sqnorm(op, prec, mass, Mk, k, L.partials, &nb);
+    if (rc > 0) return rc;
+    if (rc == 0) {
+      k_cg_fold_alpha<<<1, RED_THREADS, 0, L.stream>>>(w.S, L.partials, nb, 1);
+    } else {
+      if (int q = apply_op(op, prec, mass, Mk, k)) return q;
+      k_cg_dot<V><<<g, RED_THREADS, 0, L.stream>>>(w.S, (const V *)k, (const V *)Mk, ne, L.partials);
+      k_cg_fold_alpha<<<1, RED_THREADS, 0, L.stream>>>(w.S, L.partials, g, 2);
+    }
     k_cg_update1<V><<<g, RED_THREADS, 0, L.stream>>>(w.S, dx, dp, (V *)r, (const V *)Mk, ne, L.partials);
     k_cg_fold_lambda<<<1, RED_THREADS, 0, L.stream>>>(w.S, L.partials, g);
     k_cg_update2<V><<<g, RED_THREADS, 0, L.stream>>>(w.S, dp, (V *)k, (const V *)r, ne);

@@ -222,6 +222,33 @@ int apply_op(int op, int prec, double mass, void *out, const void *in) {
   return HRGPU_E_ARG;
 }
 
+// The even-odd H^2 (op G5DPHI_EOPRE_SQ or G5CPHI_EOPRE_SQ), the same launches
+// as apply_op, with the |H in|^2 partial sums of the first H application (one
+// per block of its last hop) in red[0 .. *nblocks): with H Hermitian,
+// <in, H^2 in> = |H in|^2, the CG's alpha without a dot-product pass.
+// Returns -1 when op has no such form (the caller takes the dot product), else
+// 0 or an error status.
+template <typename R>
+static int sq_eo_sqnorm(bool clover, double m, void *out, const void *in, double *red, int *nblocks) {
+  void **tmp = sizeof(R) == 8 ? &L.tmp_e : &L.tmp_e_f;
+  if (int rc = ensure_tmp(tmp, spinor_bytes(HRGPU_EVEN, sizeof(R) == 8 ? HRGPU_DOUBLE : HRGPU_FLOAT))) return rc;
+  if (int rc = clover ? Cphi_eo<R>(m, *tmp, in, 1, red) : Dphi_eo<R>(m, *tmp, in, HRGPU_EVEN, 1, red)) return rc;
+  // the block count of the variant that ran (tuned now if it was the first launch)
+  const int pi = sizeof(R) == 8 ? 0 : (L.flt_links == HRGPU_LINKS_BF16 ? 2 : 1);
+  const int ep = clover ? EP_CLOV : EP_AXPY;
+  const int v = L.hop_force >= 0 ? L.hop_force : L.hop_variant[pi][ep];
+  const long threads = (v & 1) ? 2L * L.VH : L.VH;
+  *nblocks = (int)((threads + HOP_THREADS - 1) / HOP_THREADS);
+  return clover ? Cphi_eo<R>(m, out, *tmp, 1, nullptr) : Dphi_eo<R>(m, out, *tmp, HRGPU_EVEN, 1, nullptr);
+}
+
+int apply_op_sqnorm(int op, int prec, double mass, void *out, const void *in, double *red, int *nblocks) {
+  if (op != HRGPU_OP_G5DPHI_EOPRE_SQ && op != HRGPU_OP_G5CPHI_EOPRE_SQ) return -1;
+  const bool clover = op == HRGPU_OP_G5CPHI_EOPRE_SQ;
+  return prec == HRGPU_DOUBLE ? sq_eo_sqnorm<double>(clover, mass, out, in, red, nblocks)
+                              : sq_eo_sqnorm<float>(clover, mass, out, in, red, nblocks);
+}
+
 int op_parity(int op) {
   return (op == HRGPU_OP_G5DPHI_SQ || op == HRGPU_OP_G5CPHI_SQ || op == HRGPU_OP_DPHI || op == HRGPU_OP_CPHI)
              ? HRGPU_FULL

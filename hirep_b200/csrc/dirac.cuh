@@ -21,6 +21,7 @@ int Dphi_eo(double m0, void *out, const void *in, int outp, int g5, double *red)
 template <typename R>
 int Cphi_eo(double mass, void *out, const void *in, int g5, double *red);
 int apply_op(int op, int prec, double mass, void *out, const void *in);
+int apply_op_sqnorm(int op, int prec, double mass, void *out, const void *in, double *red, int *nblocks);
 int op_parity(int op);
 double static_mass();
 void add_mvm(unsigned long n);  // hops done outside hop(), e.g. replayed CUDA graphs
