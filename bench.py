@@ -340,7 +340,7 @@ def hop_tuning(lat, G):
     for prec in (G.DOUBLE, G.FLOAT):
         for ep in range(3):
             chosen = G.ctypes.c_int(-1)
-            ms = (G.ctypes.c_float * 5)()
+            ms = (G.ctypes.c_float * 6)()
             G._check(lat.L.hrgpu_hop_tuning(prec, ep, G.ctypes.byref(chosen), ms), "hop_tuning")
             if chosen.value >= 0:
                 out[("f64" if prec == G.DOUBLE else "f32") + "_" + names[ep]] = {

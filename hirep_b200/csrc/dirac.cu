@@ -237,7 +237,7 @@ static int sq_eo_sqnorm(bool clover, double m, void *out, const void *in, double
   const int pi = sizeof(R) == 8 ? 0 : (L.flt_links == HRGPU_LINKS_BF16 ? 2 : 1);
   const int ep = clover ? EP_CLOV : EP_AXPY;
   const int v = L.hop_force >= 0 ? L.hop_force : L.hop_variant[pi][ep];
-  const long threads = (v & 1) ? 2L * L.VH : L.VH;
+  const long threads = hop_threads_per_site(v) * (long)L.VH;
   *nblocks = (int)((threads + HOP_THREADS - 1) / HOP_THREADS);
   return clover ? Cphi_eo<R>(m, out, *tmp, 1, nullptr) : Dphi_eo<R>(m, out, *tmp, HRGPU_EVEN, 1, nullptr);
 }

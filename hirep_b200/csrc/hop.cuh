@@ -221,10 +221,35 @@ __device__ __forceinline__ void clover_epilogue(V (&ra)[NA], V (&rb)[NA], const 
   }
 }
 
+// the t+-1 neighbours staged in shared memory by k_hop_tma: wait (bounded) for
+// the bulk copies on the block's mbarrier; false if they did not land in time
+__device__ __forceinline__ bool tma_wait(unsigned bar) {
+  for (int it = 0; it < (1 << 22); it++) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(0u)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+template <typename V>
+__device__ __forceinline__ V ld_sel(const V *p, bool smem) {
+  return smem ? *p : ld_c(p);
+}
+
 // one output site (checkerboard index cb < VH) of the hop; returns |out|^2 when a.red is set
 // LE: the storage type of a link element (BF16 for the FP32 operator's optional link copy)
-template <int NFT, bool REAL, typename R, int EP, typename LE = typename LinkE<REAL, R>::T>
-__device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb) {
+// TSM: the t+1 / t-1 neighbours come from shared memory (tsu, tsd: this thread's
+// element of component 0, components HOP_THREADS apart) once the bulk copies on
+// the mbarrier at shared address bar have landed; the t direction is then
+// visited last, after x, y, z, to give the copies time
+template <int NFT, bool REAL, typename R, int EP, typename LE = typename LinkE<REAL, R>::T, bool TSM = false>
+__device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb, const typename C2<R>::T *tsu = nullptr,
+                                           const typename C2<R>::T *tsd = nullptr, unsigned bar = 0) {
   typedef typename C2<R>::T V;
   typedef LE E;
   constexpr int NA = NFT;
@@ -244,7 +269,9 @@ __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb) {
     for (int i = 0; i < NA; i++) r0[i] = r1[i] = r2[i] = r3[i] = cmk<V>(0.0, 0.0);
     const long so = (long)outp * g.ld + cb;  // this site in the link planes
 #pragma unroll
-    for (int mu = 0; mu < 4; mu++) {
+    for (int k = 0; k < 4; k++) {
+      const int mu = TSM ? ((k + 1) & 3) : k;
+      const bool use_sm = TSM && mu == 0 && tma_wait(bar);
       int tp = t, xp = x, yp = y, zp = z, tm = t, xm = x, ym = y, zm = z;
       if (mu == 0) { tp = (t + 1 == g.T) ? 0 : t + 1; tm = (t == 0) ? g.T - 1 : t - 1; }
       if (mu == 1) { xp = (x + 1 == g.X) ? 0 : x + 1; xm = (x == 0) ? g.X - 1 : x - 1; }
@@ -255,12 +282,13 @@ __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb) {
       const E *Umu = U + (long)mu * nf2 * lplane;
       // ---- forward: (1 - gamma_mu) U(x,mu) psi(x+mu)
       {
-        const V *s = in + cup;
+        const V *s = use_sm ? tsu : in + cup;
+        const long st = use_sm ? (long)HOP_THREADS : ld;
 #pragma unroll
         for (int i = 0; i < NA; i++) {
           if (i >= nf) break;
-          V s0 = ld_c(s + (long)(0 * nf + i) * ld), s1 = ld_c(s + (long)(1 * nf + i) * ld);
-          V s2 = ld_c(s + (long)(2 * nf + i) * ld), s3 = ld_c(s + (long)(3 * nf + i) * ld);
+          V s0 = ld_sel(s + (long)(0 * nf + i) * st, use_sm), s1 = ld_sel(s + (long)(1 * nf + i) * st, use_sm);
+          V s2 = ld_sel(s + (long)(2 * nf + i) * st, use_sm), s3 = ld_sel(s + (long)(3 * nf + i) * st, use_sm);
           if (mu == 0) { h0[i] = cadd(s0, s2); h1[i] = cadd(s1, s3); }
           if (mu == 1) { h0[i] = caddi(s0, s3); h1[i] = caddi(s1, s2); }
           if (mu == 2) { h0[i] = cadd(s0, s3); h1[i] = csub(s1, s2); }
@@ -281,12 +309,13 @@ __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb) {
       }
       // ---- backward: (1 + gamma_mu) U(x-mu,mu)^+ psi(x-mu)
       {
-        const V *s = in + cdn;
+        const V *s = use_sm ? tsd : in + cdn;
+        const long st = use_sm ? (long)HOP_THREADS : ld;
 #pragma unroll
         for (int i = 0; i < NA; i++) {
           if (i >= nf) break;
-          V s0 = ld_c(s + (long)(0 * nf + i) * ld), s1 = ld_c(s + (long)(1 * nf + i) * ld);
-          V s2 = ld_c(s + (long)(2 * nf + i) * ld), s3 = ld_c(s + (long)(3 * nf + i) * ld);
+          V s0 = ld_sel(s + (long)(0 * nf + i) * st, use_sm), s1 = ld_sel(s + (long)(1 * nf + i) * st, use_sm);
+          V s2 = ld_sel(s + (long)(2 * nf + i) * st, use_sm), s3 = ld_sel(s + (long)(3 * nf + i) * st, use_sm);
           if (mu == 0) { h0[i] = csub(s0, s2); h1[i] = csub(s1, s3); }
           if (mu == 1) { h0[i] = csubi(s0, s3); h1[i] = csubi(s1, s2); }
           if (mu == 2) { h0[i] = csub(s0, s3); h1[i] = cadd(s1, s2); }
@@ -348,6 +377,10 @@ __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb) {
   }
   return nrm;
 }
+
+// threads per output site of a single-field hop variant: 2 for the spin-split
+// variants 1 and 3, 1 for the others (0, 2, 4 and 5)
+__host__ __device__ constexpr int hop_threads_per_site(int variant) { return (variant == 1 || variant == 3) ? 2 : 1; }
 
 // Programmatic dependent launch: let the next kernel of the stream be scheduled
 // as soon as every block of this one has started (its blocks then fill the SMs

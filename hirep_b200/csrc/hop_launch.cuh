@@ -4,6 +4,7 @@
 #pragma once
 #include "dirac.cuh"
 #include "hop_async.cuh"
+#include "hop_tma.cuh"
 
 namespace hrgpu {
 
@@ -47,15 +48,36 @@ int launch_async(HopArgs<R> &a, dim3 grid, dim3 block, cudaStream_t s) {
   }
 }
 
+// variant 5: the time halo staged by bulk copies, for the small representations
+// and where blocks of HOP_THREADS sites tile the time slabs of the launch
+template <int N, bool RL, typename R, int EP>
+int launch_tma(HopArgs<R> &a, dim3 grid, dim3 block, cudaStream_t s) {
+  if constexpr (AsyncOK<N, RL>::v) {
+    const int S = a.g.Xh * a.g.Y * a.g.Z;
+    if (S % HOP_THREADS != 0 || a.cb0 % HOP_THREADS != 0 || (a.cb1 - a.cb0) % HOP_THREADS != 0) return -1;
+    constexpr int smem = TmaLayout<N, R>::SMEM;
+    static bool attr = false;
+    if (!attr) {
+      HR_CUDA(cudaFuncSetAttribute(k_hop_tma<N, RL, R, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      attr = true;
+    }
+    HR_CUDA(launch_pdl<R>(k_hop_tma<N, RL, R, EP>, grid, block, smem, s, a));
+    return 0;
+  } else {
+    return -1;  // not built for this NF
+  }
+}
+
 template <typename R, int EP>
 int launch_ep_variant(HopArgs<R> &a, int variant) {
   a.g = make_geo();
   a.nf = L.nf;
   // variants: 0 one thread per site, 1 two threads per site (spin split),
   // 2 and 3 the same with the register budget capped for 4 resident blocks per SM,
-  // 4 one thread per site with the per-direction loads pipelined through shared memory
+  // 4 one thread per site with the per-direction loads pipelined through shared memory,
+  // 5 one thread per site with the time halo staged by bulk (TMA) copies
   const long nsites = a.cb1 - a.cb0;
-  const long threads = (variant & 1) ? 2L * nsites : nsites;
+  const long threads = hop_threads_per_site(variant) * nsites;
   dim3 grid((unsigned)((threads + HOP_THREADS - 1) / HOP_THREADS)), block(HOP_THREADS);
   cudaStream_t s = L.stream;
 #define HOPV(N, RL)                                                                    \
@@ -65,8 +87,11 @@ int launch_ep_variant(HopArgs<R> &a, int variant) {
       case 1: HR_CUDA(launch_pdl<R>(k_hop2<N, RL, R, EP, 1>, grid, block, 0, s, a)); break; \
       case 2: HR_CUDA(launch_pdl<R>(k_hop<N, RL, R, EP, 4>, grid, block, 0, s, a)); break;  \
       case 3: HR_CUDA(launch_pdl<R>(k_hop2<N, RL, R, EP, 4>, grid, block, 0, s, a)); break; \
-      default:                                                                         \
+      case 4:                                                                          \
         if (int rc_ = launch_async<N, RL, R, EP>(a, grid, block, s)) return rc_;       \
+        break;                                                                         \
+      default:                                                                         \
+        if (int rc_ = launch_tma<N, RL, R, EP>(a, grid, block, s)) return rc_;         \
         break;                                                                         \
     }                                                                                  \
     break;

@@ -48,7 +48,7 @@ int fail_cuda(cudaError_t e, const char *what, const char *file, int line);
 constexpr int MAXNF = 64;
 constexpr int RED_THREADS = 256;
 constexpr int RED_MAX_BLOCKS = 1184;  // 8 x 148 SMs
-constexpr int HOP_VARIANTS = 5;
+constexpr int HOP_VARIANTS = 6;
 constexpr int HOPB_VARIANTS = 3;   // batch hopping kernel variants
 constexpr int HOPB_MAXNB = 64;     // fields per batch
 

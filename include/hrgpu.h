@@ -137,18 +137,20 @@ int hrgpu_g5Dphi_eopre_flt(double m0, void *out, const void *in);
 int hrgpu_g5Dphi_eopre_sq_flt(double m0, void *out, const void *in);
 /* Hopping-kernel variant: 0 = one thread per site, 1 = two threads per site
  * (spin split), 2 and 3 = the same with registers capped for 4 blocks per SM,
- * 4 = one thread per site with cp.async-pipelined loads (NF <= 4 complex, NF = 3
- * real), -1 = autotune on first use (default).  hrgpu_hop_tuning reports the
+ * 4 = one thread per site with cp.async-pipelined loads, 5 = one thread per site
+ * with the time halo staged in shared memory by bulk (TMA) copies (4 and 5: NF <= 4
+ * complex, NF = 3 real; 5 also needs time slabs of a multiple of 128 sites per
+ * parity), -1 = autotune on first use (default).  hrgpu_hop_tuning reports the
  * variant chosen for (precision, epilogue 0..2) and the per-launch times it
- * measured (ms has room for 5 values; -1 marks a variant not built for this NF);
- * precision 2 is the FP32 operator reading BF16 links.
+ * measured (ms has room for 6 values; -1 marks a variant not built for this
+ * NF or lattice); precision 2 is the FP32 operator reading BF16 links.
  * Tuning controls of this library; they have no counterpart in the reference. */
+int hrgpu_set_hop_variant(int variant);
+int hrgpu_hop_tuning(int prec, int epilogue, int *chosen, float *ms);
 /* whole-lattice FP64 hopping kernels launched with programmatic dependent
  * launch (default 1: the next hop's blocks start in the SMs the previous hop's
  * last wave leaves idle); 0 launches them plainly */
 int hrgpu_set_hop_pdl(int on);
-int hrgpu_set_hop_variant(int variant);
-int hrgpu_hop_tuning(int prec, int epilogue, int *chosen, float *ms);
 /* Storage of the links read by the FP32 operators (the _flt operators, the
  * inner solves of cg_mshift_flt): HRGPU_LINKS_F32 (default, assign_ud2u_f's
  * copy) or HRGPU_LINKS_BF16 (a BF16 copy rounded from the FP64 links, FP32

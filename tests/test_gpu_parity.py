@@ -287,11 +287,12 @@ def test_force_matches_oracle(ng, rep, clover):
     assert rel(fg - mom, fo - mom) < 1e-12
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
 @pytest.mark.parametrize("ng,rep", [(3, O.FUND), (2, O.ADJ), (3, O.SYM)])
 def test_hop_variants(variant, ng, rep):
-    """Every variant of the hopping kernel the autotuner can pick gives the oracle's result."""
-    o, lat, _, _ = setup((4, 4, 6, 4), ng, rep, seed=21, smooth=0.3)
+    """Every variant of the hopping kernel the autotuner can pick gives the oracle's
+    result (4x16x8x4: a time slab of one parity is 256 sites, as variant 5 needs)."""
+    o, lat, _, _ = setup((4, 16, 8, 4), ng, rep, seed=21, smooth=0.3)
     G._check(lat.L.hrgpu_set_hop_variant(variant), "set_hop_variant")
     try:
         m = -0.2
