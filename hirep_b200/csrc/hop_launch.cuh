@@ -172,29 +172,38 @@ int launch_ep(HopArgs<R> &a) {
     int bestv = 0;
     cudaEvent_t e0, e1;
     HR_CUDA(cudaEventCreate(&e0));
-    HR_CUDA(cudaEventCreate(&e1));
-    for (int cand = 0; cand < HOP_VARIANTS; cand++) {
-      int rc0 = launch_ep_variant<R, EP>(a, cand);  // warm-up
-      if (rc0 < 0) {  // variant not built for this NF
-        L.hop_tune_ms[pi][EP][cand] = -1.0f;
-        continue;
-      }
-      if (rc0) return rc0;
-      HR_CUDA(cudaEventRecord(e0, L.stream));
-      for (int r = 0; r < 3; r++)
-        if (int rc = launch_ep_variant<R, EP>(a, cand)) return rc;
-      HR_CUDA(cudaEventRecord(e1, L.stream));
-      HR_CUDA(cudaEventSynchronize(e1));
-      float ms = 0;
-      HR_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-      L.hop_tune_ms[pi][EP][cand] = ms / 3.0f;
-      if (ms < best) {
-        best = ms;
-        bestv = cand;
-      }
+    if (cudaError_t err = cudaEventCreate(&e1)) {
+      cudaEventDestroy(e0);
+      return fail_cuda(err, "cudaEventCreate(&e1)", __FILE__, __LINE__);
     }
+    // the events are destroyed on every way out of the loop
+    auto tune = [&]() -> int {
+      for (int cand = 0; cand < HOP_VARIANTS; cand++) {
+        int rc0 = launch_ep_variant<R, EP>(a, cand);  // warm-up
+        if (rc0 < 0) {  // variant not built for this NF
+          L.hop_tune_ms[pi][EP][cand] = -1.0f;
+          continue;
+        }
+        if (rc0) return rc0;
+        HR_CUDA(cudaEventRecord(e0, L.stream));
+        for (int r = 0; r < 3; r++)
+          if (int rc = launch_ep_variant<R, EP>(a, cand)) return rc;
+        HR_CUDA(cudaEventRecord(e1, L.stream));
+        HR_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        HR_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        L.hop_tune_ms[pi][EP][cand] = ms / 3.0f;
+        if (ms < best) {
+          best = ms;
+          bestv = cand;
+        }
+      }
+      return 0;
+    };
+    const int trc = tune();
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (trc) return trc;
     v = bestv;
   }
   int rc = launch_ep_variant<R, EP>(a, v);
