@@ -318,18 +318,9 @@ __global__ void __launch_bounds__(BTHREADS) k_bdot(const int *state, const V *a,
 // sum over the nblk partial rows of field f (row stride nbp = 4 * tiles), fixed
 // tree order (one block)
 __device__ double bfold_one(const double *part, int nblk, int nbp, int f) {
-  __shared__ double sh[BTHREADS];
   double s = 0.0;
   for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += part[(long)b * nbp + f];
-  sh[threadIdx.x] = s;
-  __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-    __syncthreads();
-  }
-  double r = sh[0];
-  __syncthreads();
-  return r;
+  return block_sum(s);
 }
 
 __global__ void k_bfold(const double *part, int nblk, int nb, double *out) {

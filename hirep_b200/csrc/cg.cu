@@ -32,18 +32,9 @@ struct CGState {
 };
 
 __device__ double fold_partials(const double *partials, int nblocks, int stride, int off) {
-  __shared__ double sh[RED_THREADS];
   double s = 0;
   for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += partials[(long)b * stride + off];
-  sh[threadIdx.x] = s;
-  __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-    __syncthreads();
-  }
-  double r = sh[0];
-  __syncthreads();
-  return r;
+  return block_sum(s);
 }
 
 // alpha = <k, Mk>; omega = -delta/alpha; z3 and the solution coefficients (cg_mshift.c:82-91)
@@ -128,14 +119,8 @@ __global__ void __launch_bounds__(RED_THREADS) k_cg_update1(CGState *S, V *const
     r[e] = rv;
     nrm += (double)rv.x * rv.x + (double)rv.y * rv.y;
   }
-  __shared__ double sh[RED_THREADS];
-  sh[threadIdx.x] = nrm;
-  __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) partials[blockIdx.x] = sh[0];
+  nrm = block_sum(nrm);
+  if (threadIdx.x == 0) partials[blockIdx.x] = nrm;
 }
 
 template <typename V>
@@ -173,15 +158,9 @@ __global__ void __launch_bounds__(RED_THREADS) k_cg_dot(const CGState *S, const 
     V u = a[e], v = b[e];
     re += (double)u.x * v.x + (double)u.y * v.y;
   }
-  __shared__ double sh[RED_THREADS];
-  sh[threadIdx.x] = re;
-  __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-    __syncthreads();
-  }
+  re = block_sum(re);
   if (threadIdx.x == 0) {
-    partials[2 * blockIdx.x] = sh[0];
+    partials[2 * blockIdx.x] = re;
     partials[2 * blockIdx.x + 1] = 0.0;
   }
 }

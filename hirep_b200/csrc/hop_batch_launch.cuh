@@ -57,24 +57,33 @@ int launch_batch(TileArgs<R> &a) {
     int bestv = 0;
     cudaEvent_t e0, e1;
     HR_CUDA(cudaEventCreate(&e0));
-    HR_CUDA(cudaEventCreate(&e1));
-    for (int cand = 0; cand < HOPB_VARIANTS; cand++) {
-      if (int rc = launch_batch_variant<R, EP>(a, cand)) return rc;
-      HR_CUDA(cudaEventRecord(e0, L.stream));
-      for (int r = 0; r < 3; r++)
-        if (int rc = launch_batch_variant<R, EP>(a, cand)) return rc;
-      HR_CUDA(cudaEventRecord(e1, L.stream));
-      HR_CUDA(cudaEventSynchronize(e1));
-      float ms = 0;
-      HR_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-      L.hopb_tune_ms[pi][EP][a.nb][cand] = ms / 3.0f;
-      if (ms < best) {
-        best = ms;
-        bestv = cand;
-      }
+    if (cudaError_t err = cudaEventCreate(&e1)) {
+      cudaEventDestroy(e0);
+      return fail_cuda(err, "cudaEventCreate(&e1)", __FILE__, __LINE__);
     }
+    // the events are destroyed on every way out of the loop
+    auto tune = [&]() -> int {
+      for (int cand = 0; cand < HOPB_VARIANTS; cand++) {
+        if (int rc = launch_batch_variant<R, EP>(a, cand)) return rc;
+        HR_CUDA(cudaEventRecord(e0, L.stream));
+        for (int r = 0; r < 3; r++)
+          if (int rc = launch_batch_variant<R, EP>(a, cand)) return rc;
+        HR_CUDA(cudaEventRecord(e1, L.stream));
+        HR_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        HR_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        L.hopb_tune_ms[pi][EP][a.nb][cand] = ms / 3.0f;
+        if (ms < best) {
+          best = ms;
+          bestv = cand;
+        }
+      }
+      return 0;
+    };
+    const int trc = tune();
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (trc) return trc;
     v = (signed char)(bestv + 1);
   }
   return launch_batch_variant<R, EP>(a, v - 1);

@@ -168,6 +168,13 @@ int launch_ep(HopArgs<R> &a) {
     return launch_ep_variant<R, EP>(a, 0);
   }
   if (v < 0) {
+    // nothing can be timed while the stream is being captured into a CUDA
+    // graph: run the default variant and leave tuning to an uncaptured launch
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    HR_CUDA(cudaStreamIsCapturing(L.stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return launch_ep_variant<R, EP>(a, 0);
+  }
+  if (v < 0) {
     float best = 1e30f;
     int bestv = 0;
     cudaEvent_t e0, e1;

@@ -171,6 +171,30 @@ template <typename V, typename R> __device__ __forceinline__ void rmac(V &acc, R
 }
 template <typename V, typename R> __device__ __forceinline__ V cscale(R r, V a) { V o; o.x = r * a.x; o.y = r * a.y; return o; }
 
+// Sum of v over the thread block in a fixed order, so the result is the same on
+// every run: a shuffle tree inside each warp, then warp 0 adds the warp sums
+// with a second shuffle tree.  Every thread gets the sum.  blockDim.x must be a
+// multiple of 32 and every thread of the block must call it.
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double warp_sums[32];
+  __shared__ double total;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if (lane == 0) warp_sums[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    double s = lane < nw ? warp_sums[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) total = s;
+  }
+  __syncthreads();
+  // a following call writes warp_sums only after this barrier and total only
+  // after its own first barrier, which every thread reaches after reading total
+  return total;
+}
+
 // ---------------------------------------------------------------------------
 // lattice coordinates on the device
 // ---------------------------------------------------------------------------

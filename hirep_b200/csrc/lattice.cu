@@ -286,18 +286,11 @@ int links_out(void *host, const void *dev, int nel, int elem_bytes, int ndir) {
 // L.partials; one block folds them in a fixed order.
 // ---------------------------------------------------------------------------
 __global__ void k_fold(double *partials, int nblocks, int nvals, double *out) {
-  __shared__ double sh[RED_THREADS];
   for (int v = 0; v < nvals; v++) {
     double s = 0;
     for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += partials[(long)b * nvals + v];
-    sh[threadIdx.x] = s;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-      if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) out[v] = sh[0];
-    __syncthreads();
+    s = block_sum(s);
+    if (threadIdx.x == 0) out[v] = s;
   }
 }
 

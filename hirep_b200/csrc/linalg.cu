@@ -108,20 +108,11 @@ __global__ void __launch_bounds__(RED_THREADS) k_dot(int op, const V *s1, const 
       im += sg * ((double)a.x * b.y - (double)a.y * b.x);
     }
   }
-  __shared__ double sr[RED_THREADS], si[RED_THREADS];
-  sr[threadIdx.x] = re;
-  si[threadIdx.x] = im;
-  __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if ((int)threadIdx.x < w) {
-      sr[threadIdx.x] += sr[threadIdx.x + w];
-      si[threadIdx.x] += si[threadIdx.x + w];
-    }
-    __syncthreads();
-  }
+  re = block_sum(re);
+  im = op == 2 ? 0.0 : block_sum(im);
   if (threadIdx.x == 0) {
-    partials[2 * blockIdx.x] = sr[0];
-    partials[2 * blockIdx.x + 1] = si[0];
+    partials[2 * blockIdx.x] = re;
+    partials[2 * blockIdx.x + 1] = im;
   }
 }
 
