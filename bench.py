@@ -507,16 +507,19 @@ def run_hmc_check(torch, G, F):
     lat = G.Lattice(*H_DIMS, H_NG, G.ADJ)
     u0 = F.smooth_gauge(H_SEED, lat.V, H_NG, H_EPS)
     out = {"workload": "SU(2) adjoint Nf=2 Wilson m0=-1.0 + plaquette beta=2.25, 32^3x64, U=exp(i0.2H) seed 99; "
-                       "O2MN tau=1, 20 steps; force solves 1e-10, accept/reject 1e-14"}
+                       "O2MN tau=1, 20 steps; force solves 1e-10, accept/reject 1e-14",
+           "draws": "momenta and pseudofermion source drawn on the device (gaussian_momenta, "
+                    "gaussian_spinor_field: Philox4x32-10, Box-Muller), inside the timed trajectory"}
     for name, solver in (("mixed", "cg_mixed"), ("fp64", "cg")):
         lat.set_gauge(u0)
         lat.represent_gauge_field(True)
         HMC(lat, H_BETA, H_MASS, tau=0.1, nsteps=2, force_err2=1e-20, mt_err2=1e-28,
-            force_solver=solver).trajectory(np.random.default_rng(H_SEED + 1), metropolis=False)
+            force_solver=solver, draws="device").trajectory(np.random.default_rng(H_SEED + 1), metropolis=False)
         lat.set_gauge(u0)
         lat.represent_gauge_field(True)
         plaq0 = lat.avr_plaquette()
-        hmc = HMC(lat, H_BETA, H_MASS, tau=1.0, nsteps=20, force_err2=1e-20, mt_err2=1e-28, force_solver=solver)
+        hmc = HMC(lat, H_BETA, H_MASS, tau=1.0, nsteps=20, force_err2=1e-20, mt_err2=1e-28, force_solver=solver,
+                  draws="device")
         torch.cuda.synchronize()
         r = hmc.trajectory(np.random.default_rng(H_SEED), metropolis=False)
         out[name] = {"seconds": r["seconds"], "dH": r["dH"], "force_solve_mvm": r["force_solve_iters"],

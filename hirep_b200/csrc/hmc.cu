@@ -14,6 +14,7 @@
 #include <math.h>
 
 #include "dirac.cuh"
+#include "rng.cuh"
 
 namespace hrgpu {
 
@@ -294,6 +295,50 @@ __global__ void k_add(double *a, const double *b, long n) {
 
 static unsigned nb128(long n) { return (unsigned)((n + 127) / 128); }
 
+// ---------------------------------------------------------------------------
+// Gaussian draws on the device (rng.cuh): the generator key is set by
+// hrgpu_random_seed, and every draw takes the next stream number, so
+// successive draws are independent and a seed replays its sequence of draws.
+// ---------------------------------------------------------------------------
+static uint32_t g_rng_key[2] = {0u, 0u};
+static uint64_t g_rng_stream = 0;
+
+static unsigned rng_grid(long n) {
+  const long b = (n + 255) / 256;
+  return (unsigned)(b < 148L * 16 ? b : 148L * 16);
+}
+
+// element e of a spinor field ([planes][ld] complex): a complex Gaussian of
+// variance 2 scale^2 at real sites, zero in the padding (cb >= VH)
+template <typename V>
+__global__ void k_gauss_spinor(V *s, long n, int ld, int VH, uint64_t stream, uint32_t k0, uint32_t k1, double scale) {
+  typedef decltype(s[0].x) R;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    V o;
+    o.x = (R)0;
+    o.y = (R)0;
+    if ((int)(e % ld) < VH) {
+      const double2 z = gauss_pair((uint64_t)e, stream, k0, k1);
+      o.x = (R)(scale * z.x);
+      o.y = (R)(scale * z.y);
+    }
+    s[e] = o;
+  }
+}
+
+// momenta [4][dimg][2 ld] doubles: entries 2q and 2q+1 (one row, as 2 ld is
+// even) take the two Gaussians of block q, times scale; padding sites stay zero
+__global__ void k_gauss_momenta(double *mom, long npairs, int ld, int VH, uint64_t stream, uint32_t k0, uint32_t k1,
+                                double scale) {
+  for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < npairs; q += (long)gridDim.x * blockDim.x) {
+    const double2 z = gauss_pair((uint64_t)q, stream, k0, k1);
+    const long d0 = (2 * q) % (2L * ld);
+    const long c0 = d0 >= ld ? d0 - ld : d0, c1 = d0 + 1 >= ld ? d0 + 1 - ld : d0 + 1;
+    mom[2 * q] = c0 < VH ? scale * z.x : 0.0;
+    mom[2 * q + 1] = c1 < VH ? scale * z.y : 0.0;
+  }
+}
+
 }  // namespace hrgpu
 
 using namespace hrgpu;
@@ -315,6 +360,44 @@ int hrgpu_momenta_get(double *host) {
   if (int rc = hmc_setup()) return rc;
   HR_REQUIRE(host, HRGPU_E_ARG, "momenta_get: NULL field");
   return links_out(host, L.mom, L.dimg, 8, 4);
+}
+
+int hrgpu_random_seed(unsigned long long seed) {
+  g_rng_key[0] = (uint32_t)seed;
+  g_rng_key[1] = (uint32_t)(seed >> 32);
+  g_rng_stream = 0;
+  return 0;
+}
+
+// gaussian_momenta (LibHR/Update/random_momenta.c:18-38): every generator
+// component N(0, 1) / sqrt(C(fund)); apply_BCs_on_momentum_field is the
+// identity for the periodic / antiperiodic boundary conditions of this library
+int hrgpu_gaussian_momenta(void) {
+  if (int rc = hmc_setup()) return rc;
+  const long n = 4L * L.dimg * 2L * L.ld;
+  k_gauss_momenta<<<rng_grid(n / 2), 256, 0, L.stream>>>(L.mom, n / 2, L.ld, (int)L.VH, g_rng_stream++, g_rng_key[0],
+                                                         g_rng_key[1], 1.0 / sqrt(L.fund_norm2));
+  HR_LAUNCH_CHECK();
+  return 0;
+}
+
+// gaussian_spinor_field (LibHR/Update/random_spinor_field.c:14-25): every real
+// component N(0, 1) / sqrt(2); the FP32 field is the FP64 draw rounded
+// (gaussian_spinor_field_flt, :27-36, draws in single precision)
+int hrgpu_gaussian_spinor_field(int par, int prec, void *s) {
+  HR_REQUIRE(L.ready, HRGPU_E_STATE, "gaussian_spinor_field: lattice not initialised");
+  HR_REQUIRE(s && par >= 0 && par <= 2 && (prec == HRGPU_DOUBLE || prec == HRGPU_FLOAT), HRGPU_E_ARG,
+             "gaussian_spinor_field: bad arguments");
+  const long n = (long)spinor_elems(par);
+  const double c1 = 1.0 / sqrt(2.0);
+  if (prec == HRGPU_DOUBLE)
+    k_gauss_spinor<double2><<<rng_grid(n), 256, 0, L.stream>>>((double2 *)s, n, L.ld, (int)L.VH, g_rng_stream++,
+                                                               g_rng_key[0], g_rng_key[1], c1);
+  else
+    k_gauss_spinor<float2><<<rng_grid(n), 256, 0, L.stream>>>((float2 *)s, n, L.ld, (int)L.VH, g_rng_stream++,
+                                                              g_rng_key[0], g_rng_key[1], c1);
+  HR_LAUNCH_CHECK();
+  return 0;
 }
 
 int hrgpu_gauge_get(double *u_host) {

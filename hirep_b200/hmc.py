@@ -75,12 +75,18 @@ def integrate(kind, nsteps, tlen, force, field):
 
 class HMC:
     def __init__(self, lat, beta, mass, tau, nsteps, force_err2=1e-20, mt_err2=1e-28, force_solver="cg_mixed",
-                 bc_t_antiperiodic=True, levels=None, mre_past=0):
+                 bc_t_antiperiodic=True, levels=None, mre_past=0, draws="host"):
         """levels: [(integrator, nsteps, monomials), ...] from the outermost level
         in; None is [("o2mn", nsteps, ("gauge", "fermion"))].  mre_past > 0: the
         force solves start from the chronological (MRE) guess over that many past
         solutions (mre.c, as force_hmc.c:122-145 uses it); 0: the g5QMR solves
-        start from zero and the CG solves from the previous solution."""
+        start from zero and the CG solves from the previous solution.  draws:
+        "host" draws the momenta and the pseudofermion source with the numpy
+        Generator passed to trajectory(); "device" draws them on the GPU
+        (gaussian_momenta, gaussian_spinor_field) with a seed taken from it."""
+        if draws not in ("host", "device"):
+            raise ValueError("draws: host or device")
+        self.draws = draws
         if force_solver not in ("cg_mixed", "cg", "g5qmr"):
             raise ValueError("force_solver: cg_mixed, cg or g5qmr")
         if levels is None:
@@ -195,9 +201,14 @@ class HMC:
         t0 = time.perf_counter()
         # momenta (random_momenta.c: gauss / sqrt(C(F))) and pseudofermion heatbath
         # (gaussian_spinor_field: gauss / sqrt(2)); the starting action holds |eta|^2
-        lat.momenta_set(rng.standard_normal((lat.V, 4, lat.dimg)) / np.sqrt(0.5))
-        eta_h = (rng.standard_normal((lat.VH, 4, lat.nf)) + 1j * rng.standard_normal((lat.VH, 4, lat.nf))) / np.sqrt(2)
-        eta = lat.field(G.EVEN, host=eta_h)
+        if self.draws == "device":
+            lat.random_seed(int(rng.integers(2**63)))
+            lat.gaussian_momenta()
+            eta = lat.gaussian_spinor_field(lat.field(G.EVEN))
+        else:
+            lat.momenta_set(rng.standard_normal((lat.V, 4, lat.dimg)) / np.sqrt(0.5))
+            eta_h = (rng.standard_normal((lat.VH, 4, lat.nf)) + 1j * rng.standard_normal((lat.VH, 4, lat.nf))) / np.sqrt(2)
+            eta = lat.field(G.EVEN, host=eta_h)
         lat.local_hmc_action(False, self.beta)
         lat.pf_local_action(eta)
         if self.logdet:

@@ -41,6 +41,7 @@ def lib():
         L.hrgpu_get_dirac_mass.restype = ctypes.c_double
         L.hrgpu_batch_bytes.restype = ctypes.c_size_t
         L.hrgpu_mre_init.restype = ctypes.c_void_p
+        L.hrgpu_random_seed.argtypes = [ctypes.c_ulonglong]
         _lib = L
     return _lib
 
@@ -348,6 +349,19 @@ class Lattice:
         mom = np.empty((self.V, 4, self.dimg), np.float64)
         _check(self.L.hrgpu_momenta_get(_ptr(mom)), "momenta_get")
         return mom
+
+    # random draws on the device (Philox4x32-10, Box-Muller) ---------------
+    def random_seed(self, seed):
+        _check(self.L.hrgpu_random_seed(int(seed) & (2**64 - 1)), "random_seed")
+
+    def gaussian_momenta(self):
+        """gaussian_momenta (random_momenta.c:18-38) into the device momenta."""
+        _check(self.L.hrgpu_gaussian_momenta(), "gaussian_momenta")
+
+    def gaussian_spinor_field(self, f):
+        """gaussian_spinor_field (random_spinor_field.c:14-36) into a device field."""
+        _check(self.L.hrgpu_gaussian_spinor_field(f.par, f.prec, f.ptr), "gaussian_spinor_field")
+        return f
 
     def gauge_get(self):
         u = np.empty((self.V, 4, self.ng, self.ng), np.complex128)

@@ -288,6 +288,20 @@ int hrgpu_mre_free(void *mre);
  * order; the library keeps one device copy. */
 int hrgpu_momenta_set(const double *host);
 int hrgpu_momenta_get(double *host);
+/* Random draws on the device.  HiRep draws with ranlux on the host
+ * (rlxd_init, LibHR/Random/ranlxd.c; gauss, LibHR/Random/gauss.c); here the
+ * generator is Philox4x32-10 with Box-Muller Gaussians, keyed by
+ * hrgpu_random_seed (the counterpart of rlxd_init's seed; a seed replays its
+ * sequence of draws).  The numbers differ from ranlux's, the distributions
+ * are the same.
+ * gaussian_momenta: LibHR/Update/random_momenta.c:18-38 (fills the device
+ * momenta: N(0,1)/sqrt(C(fund)) per generator component).
+ * gaussian_spinor_field: LibHR/Update/random_spinor_field.c:14-36 (N(0,1)/sqrt(2)
+ * per real component of a device field of parity par; FP32: the FP64 draw
+ * rounded); padding sites are zero. */
+int hrgpu_random_seed(unsigned long long seed);
+int hrgpu_gaussian_momenta(void);
+int hrgpu_gaussian_spinor_field(int par, int prec, void *s);
 /* the fundamental links, host layout of hrgpu_gauge_set */
 int hrgpu_gauge_get(double *u_host);
 /* force0 (LibHR/Update/force0.c:22-99): momenta += -dt beta/NG proj(U staples^+) */
