@@ -509,7 +509,8 @@ def run_hmc_check(torch, G, F):
     out = {"workload": "SU(2) adjoint Nf=2 Wilson m0=-1.0 + plaquette beta=2.25, 32^3x64, U=exp(i0.2H) seed 99; "
                        "O2MN tau=1, 20 steps; force solves 1e-10, accept/reject 1e-14",
            "draws": "momenta and pseudofermion source drawn on the device (gaussian_momenta, "
-                    "gaussian_spinor_field: Philox4x32-10, Box-Muller), inside the timed trajectory"}
+                    "gaussian_spinor_field: Philox4x32-10, Box-Muller), inside the timed trajectory",
+           "accept_reject": "correct_la_pf as FP64 CG on H^2 then H (accept_reject_mvm counts H^2 applications)"}
     for name, solver in (("mixed", "cg_mixed"), ("fp64", "cg")):
         lat.set_gauge(u0)
         lat.represent_gauge_field(True)

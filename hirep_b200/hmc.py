@@ -75,7 +75,7 @@ def integrate(kind, nsteps, tlen, force, field):
 
 class HMC:
     def __init__(self, lat, beta, mass, tau, nsteps, force_err2=1e-20, mt_err2=1e-28, force_solver="cg_mixed",
-                 bc_t_antiperiodic=True, levels=None, mre_past=0, draws="host"):
+                 bc_t_antiperiodic=True, levels=None, mre_past=0, draws="host", mt_solver="cg"):
         """levels: [(integrator, nsteps, monomials), ...] from the outermost level
         in; None is [("o2mn", nsteps, ("gauge", "fermion"))].  mre_past > 0: the
         force solves start from the chronological (MRE) guess over that many past
@@ -83,7 +83,15 @@ class HMC:
         start from zero and the CG solves from the previous solution.  draws:
         "host" draws the momenta and the pseudofermion source with the numpy
         Generator passed to trajectory(); "device" draws them on the GPU
-        (gaussian_momenta, gaussian_spinor_field) with a seed taken from it."""
+        (gaussian_momenta, gaussian_spinor_field) with a seed taken from it.
+        mt_solver: the accept/reject solve pf <- H^-1 pf (correct_la_pf), FP64 at
+        mt_err2: "g5qmr" is HiRep's g5QMR on D with source g5 pf; "cg" solves
+        H^2 y = pf and sets pf = H y, the same equation H x = pf with the same
+        residual (H x - pf = H^2 y - pf), in about half the hopping-term
+        applications on the captured CG iterations."""
+        if mt_solver not in ("cg", "g5qmr"):
+            raise ValueError("mt_solver: cg or g5qmr")
+        self.mt_solver = mt_solver
         if draws not in ("host", "device"):
             raise ValueError("draws: host or device")
         self.draws = draws
@@ -220,10 +228,17 @@ class HMC:
         self.md()
         lat.project_gauge_field()
         lat.represent_gauge_field(self.bc)
-        # correct_la_pf: pf <- H^-1 pf = D^-1 g5 pf (g5QMR, FP64, MT precision)
-        lat.la("g5", self.tmp, self.pf)
-        lat.la("zero", self.pf)
-        it, ok = lat.g5QMR_mshift(self.op_d, self.mass, [0.0], self.mt_err2, self.tmp, [self.pf])
+        # correct_la_pf: pf <- H^-1 pf (FP64, MT precision)
+        if self.mt_solver == "g5qmr":
+            # D^-1 g5 pf by g5QMR, as HiRep
+            lat.la("g5", self.tmp, self.pf)
+            lat.la("zero", self.pf)
+            it, ok = lat.g5QMR_mshift(self.op_d, self.mass, [0.0], self.mt_err2, self.tmp, [self.pf])
+        else:
+            # H^2 y = pf by CG from zero, then pf = H y
+            lat.la("zero", self.tmp)
+            it, ok = lat.cg_mshift(self.op_h2, self.mass, [0.0], self.mt_err2, self.pf, [self.tmp])
+            self.apply_h(self.mass, self.pf, self.tmp)
         if not ok:
             raise G.HRGPUError("HMC: accept/reject solve did not converge")
         lat.local_hmc_action(True, self.beta)

@@ -279,3 +279,23 @@ def test_hmc_energy_violation_scales_as_dt_squared():
         hmc = HMC(lat, beta, mass, tau=0.5, nsteps=n, force_err2=1e-26, force_solver="cg")
         dh[n] = hmc.trajectory(np.random.default_rng(8), metropolis=False)["dH"]
     assert 3.5 < dh[16] / dh[32] < 4.5, dh  # the oracle trajectory gives 3.97 here
+
+
+def test_hmc_accept_reject_solver_forms_agree():
+    """correct_la_pf as HiRep's g5QMR on D and as CG on H^2 followed by H: the
+    same equation H x = pf to the same residual, so the same dH (clover, so
+    that both the log-det and the operator enter)."""
+    from hirep_b200.hmc import HMC
+
+    dims, ng, beta, mass = (4, 4, 4, 4), 3, 5.6, -0.3
+    u0 = F.smooth_gauge(97, 256, ng, 0.2)
+    out = {}
+    for s in ("g5qmr", "cg"):
+        lat = G.Lattice(*dims, ng, G.FUND)
+        lat.set_gauge(u0)
+        lat.represent_gauge_field(True)
+        lat.clover_init(1.2)
+        hmc = HMC(lat, beta, mass, tau=0.5, nsteps=10, force_err2=1e-24, mt_err2=1e-28, force_solver="cg",
+                  mt_solver=s)
+        out[s] = hmc.trajectory(np.random.default_rng(6), metropolis=False)["dH"]
+    assert abs(out["cg"] - out["g5qmr"]) < 1e-9 * max(1.0, abs(out["g5qmr"])), out
