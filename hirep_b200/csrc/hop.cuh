@@ -40,6 +40,7 @@ struct HopArgs {
   int g5;
   int nf;
   int cb0, cb1;      // output sites cb0 <= cb < cb1 of parity outp
+  int recon;         // Lattice::recon12 at launch: 2 puts the antiperiodic sign on rebuilt rows
   Geo g;
 };
 
@@ -134,6 +135,43 @@ __device__ __forceinline__ void link_mul(float2 *chi, const float2 *h, const __n
     }
     chi[i] = a;
   }
+}
+
+// c0 = W h0 and c1 = W h1 with W = U (DAG=false) or U^+ (DAG=true) of one link.
+// R12 (complex NF = 3 links stored in the operator's own precision, in the
+// kernels instantiated for reconstruction): only rows 0 and 1 are loaded and
+// row 2 is rebuilt as sg conj(r0 x r1) (su3_row2), a third less link traffic;
+// otherwise the full link is read.
+template <int NA, bool DAG, bool R12, typename V, typename E, typename R>
+__device__ __forceinline__ void link_mul2(V *c0, V *c1, const V *h0, const V *h1, const E *U, long plane, long site,
+                                          int nf, R sg) {
+  if constexpr (R12) {
+    {
+      V u[9];
+#pragma unroll
+      for (int e = 0; e < 6; e++) u[e] = ld_c(U + (long)e * plane + site);
+      su3_row2(u, sg);
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        V a0 = cmk<V>(0.0, 0.0), a1 = cmk<V>(0.0, 0.0);
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+          if (!DAG) {
+            cmac(a0, u[3 * i + j], h0[j]);
+            cmac(a1, u[3 * i + j], h1[j]);
+          } else {
+            cmacc(a0, u[3 * j + i], h0[j]);
+            cmacc(a1, u[3 * j + i], h1[j]);
+          }
+        }
+        c0[i] = a0;
+        c1[i] = a1;
+      }
+      return;
+    }
+  }
+  link_mul<NA, DAG>(c0, h0, U, plane, site, nf);
+  link_mul<NA, DAG>(c1, h1, U, plane, site, nf);
 }
 
 // BF16 storage type of a link element
@@ -247,12 +285,14 @@ __device__ __forceinline__ V ld_sel(const V *p, bool smem) {
 // element of component 0, components HOP_THREADS apart) once the bulk copies on
 // the mbarrier at shared address bar have landed; the t direction is then
 // visited last, after x, y, z, to give the copies time
-template <int NFT, bool REAL, typename R, int EP, typename LE = typename LinkE<REAL, R>::T, bool TSM = false>
+template <int NFT, bool REAL, typename R, int EP, typename LE = typename LinkE<REAL, R>::T, bool TSM = false,
+          bool RC = false>
 __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb, const typename C2<R>::T *tsu = nullptr,
                                            const typename C2<R>::T *tsd = nullptr, unsigned bar = 0) {
   typedef typename C2<R>::T V;
   typedef LE E;
   constexpr int NA = NFT;
+  constexpr bool R12 = RC && NFT == 3 && !REAL && std::is_same<LE, V>::value;
   const int nf = NFT;
   const Geo g = a.g;
   double nrm = 0.0;
@@ -294,8 +334,8 @@ __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb, co
           if (mu == 2) { h0[i] = cadd(s0, s3); h1[i] = csub(s1, s2); }
           if (mu == 3) { h0[i] = caddi(s0, s2); h1[i] = csubi(s1, s3); }
         }
-        link_mul<NA, false>(c0, h0, Umu, lplane, so, nf);
-        link_mul<NA, false>(c1, h1, Umu, lplane, so, nf);
+        const R sgf = (a.recon == 2 && mu == 0 && t == 0) ? (R)-1 : (R)1;
+        link_mul2<NA, false, R12>(c0, c1, h0, h1, Umu, lplane, so, nf, sgf);
 #pragma unroll
         for (int i = 0; i < NA; i++) {
           if (i >= nf) break;
@@ -322,8 +362,8 @@ __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb, co
           if (mu == 3) { h0[i] = csubi(s0, s2); h1[i] = caddi(s1, s3); }
         }
         const long sn = (long)inp * g.ld + cdn;
-        link_mul<NA, true>(c0, h0, Umu, lplane, sn, nf);
-        link_mul<NA, true>(c1, h1, Umu, lplane, sn, nf);
+        const R sgb = (a.recon == 2 && mu == 0 && tm == 0) ? (R)-1 : (R)1;
+        link_mul2<NA, true, R12>(c0, c1, h0, h1, Umu, lplane, sn, nf, sgb);
 #pragma unroll
         for (int i = 0; i < NA; i++) {
           if (i >= nf) break;
@@ -392,13 +432,14 @@ __device__ __forceinline__ void pdl_enter() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
-template <int NFT, bool REAL, typename R, int EP, int MINB, typename LE = typename LinkE<REAL, R>::T>
+// RC: rebuild row 2 of the SU(3) links (instantiated for complex NF = 3 only)
+template <int NFT, bool REAL, typename R, int EP, int MINB, typename LE = typename LinkE<REAL, R>::T, bool RC = false>
 __global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop(HopArgs<R> a) {
   pdl_enter();
   if (a.stop && *a.stop) return;
   const int cb = a.cb0 + blockIdx.x * blockDim.x + threadIdx.x;
   double nrm = 0.0;
-  if (cb < a.cb1) nrm = hop_site<NFT, REAL, R, EP, LE>(a, cb);
+  if (cb < a.cb1) nrm = hop_site<NFT, REAL, R, EP, LE, false, RC>(a, cb);
   if (a.red) block_partial<R>(nrm, a.red);
 }
 

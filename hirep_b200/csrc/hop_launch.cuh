@@ -68,10 +68,21 @@ int launch_tma(HopArgs<R> &a, dim3 grid, dim3 block, cudaStream_t s) {
   }
 }
 
+// k_hop for variants 0 and 2: the instantiation that rebuilds row 2 of the
+// SU(3) links when the links passed the check, else the one reading full links
+template <int N, bool RL, typename R, int EP, int MINB>
+static inline void (*hop_kernel(int recon))(HopArgs<R>) {
+  if constexpr (N == 3 && !RL) {
+    if (recon) return k_hop<N, RL, R, EP, MINB, typename LinkE<RL, R>::T, true>;
+  }
+  return k_hop<N, RL, R, EP, MINB>;
+}
+
 template <typename R, int EP>
 int launch_ep_variant(HopArgs<R> &a, int variant) {
   a.g = make_geo();
   a.nf = L.nf;
+  a.recon = L.recon_allow ? L.recon12 : 0;
   // variants: 0 one thread per site, 1 two threads per site (spin split),
   // 2 and 3 the same with the register budget capped for 4 resident blocks per SM,
   // 4 one thread per site with the per-direction loads pipelined through shared memory,
@@ -83,9 +94,9 @@ int launch_ep_variant(HopArgs<R> &a, int variant) {
 #define HOPV(N, RL)                                                                    \
   case N:                                                                              \
     switch (variant) {                                                                 \
-      case 0: HR_CUDA(launch_pdl<R>(k_hop<N, RL, R, EP, 1>, grid, block, 0, s, a)); break;  \
+      case 0: HR_CUDA(launch_pdl<R>(hop_kernel<N, RL, R, EP, 1>(a.recon), grid, block, 0, s, a)); break; \
       case 1: HR_CUDA(launch_pdl<R>(k_hop2<N, RL, R, EP, 1>, grid, block, 0, s, a)); break; \
-      case 2: HR_CUDA(launch_pdl<R>(k_hop<N, RL, R, EP, 4>, grid, block, 0, s, a)); break;  \
+      case 2: HR_CUDA(launch_pdl<R>(hop_kernel<N, RL, R, EP, 4>(a.recon), grid, block, 0, s, a)); break; \
       case 3: HR_CUDA(launch_pdl<R>(k_hop2<N, RL, R, EP, 4>, grid, block, 0, s, a)); break; \
       case 4:                                                                          \
         if (int rc_ = launch_async<N, RL, R, EP>(a, grid, block, s)) return rc_;       \

@@ -85,6 +85,11 @@ struct Lattice {
   double *force_sum = nullptr;    // [4][dimg][2*ld]
   double *mom = nullptr;          // momenta [4][dimg][2*ld]
   int bc_t = 1;                   // time boundary condition of the last represent_gauge_field
+  // hopping kernels rebuild row 2 of each SU(3) link from rows 0 and 1: 0 no
+  // (full loads), 1 yes, 2 yes with the antiperiodic-T sign on mu = 0 links at
+  // t = 0 (set by represent_gauge_field after checking every link)
+  int recon12 = 0;
+  bool recon_allow = true;        // hrgpu_set_link_recon
   double2 *cl_force = nullptr;    // [6][nf*nf][2*ld]
   // algebra projection tables (sparse): for each generator A, entries (k=i*nf+j, coeff)
   int *d_proj_off = nullptr;      // [dimg+1]
@@ -170,6 +175,24 @@ template <typename V, typename R> __device__ __forceinline__ void rmac(V &acc, R
   acc.x = fma(r, s.x, acc.x); acc.y = fma(r, s.y, acc.y);
 }
 template <typename V, typename R> __device__ __forceinline__ V cscale(R r, V a) { V o; o.x = r * a.x; o.y = r * a.y; return o; }
+template <typename V> __device__ __forceinline__ V cmul(V a, V b) {
+  V r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
+}
+
+// Row 2 of a unitary 3x3 link with determinant s from rows 0 and 1 (elements
+// u[0..5], row-major): u[6..8] = s conj(r0 x r1).  For U in SU(3) (s = 1), and
+// for -U (s = -1, a link that carries the antiperiodic time sign), this is the
+// stored row to rounding.
+template <typename V, typename R>
+__device__ __forceinline__ void su3_row2(V *u, R s) {
+  V q;
+  q = csub(cmul(u[1], u[5]), cmul(u[2], u[4]));
+  u[6].x = s * q.x; u[6].y = -s * q.y;
+  q = csub(cmul(u[2], u[3]), cmul(u[0], u[5]));
+  u[7].x = s * q.x; u[7].y = -s * q.y;
+  q = csub(cmul(u[0], u[4]), cmul(u[1], u[3]));
+  u[8].x = s * q.x; u[8].y = -s * q.y;
+}
 
 // Sum of v over the thread block in a fixed order, so the result is the same on
 // every run: a shuffle tree inside each warp, then warp 0 adds the warp sums

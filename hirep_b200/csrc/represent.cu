@@ -121,11 +121,65 @@ __global__ void k_represent(void *Uout, const double2 *Ug, int ng, int repr, Geo
 #undef MF
 }
 
+
+// bad = 1 when row 2 of some link differs from s conj(r0 x r1) by more than tol
+// (s = -1 on the links that carry the antiperiodic time sign); grid: sites of
+// both parities x 4 directions
+__global__ void k_check_row2(const double2 *U, Geo g, int bc, double tol, int *bad) {
+  const long d = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int mu = blockIdx.y;
+  if (d >= 2L * g.ld) return;
+  const int p = d >= g.ld ? 1 : 0, cb = (int)(d - (long)p * g.ld);
+  if (cb >= g.VH) return;
+  int t, x, y, z;
+  cb_to_coords(g, cb, p, t, x, y, z);
+  const long plane = 2L * g.ld;
+  const double2 *Um = U + (long)mu * 9 * plane + d;
+  double2 u[9];
+  for (int e = 0; e < 9; e++) u[e] = Um[(long)e * plane];
+  const double2 r6 = u[6], r7 = u[7], r8 = u[8];
+  su3_row2(u, (bc && mu == 0 && t == 0) ? -1.0 : 1.0);
+  double dev = fmax(fmax(fabs(u[6].x - r6.x), fabs(u[6].y - r6.y)), fmax(fabs(u[7].x - r7.x), fabs(u[7].y - r7.y)));
+  dev = fmax(dev, fmax(fabs(u[8].x - r8.x), fabs(u[8].y - r8.y)));
+  if (!(dev <= tol)) atomicOr(bad, 1);  // NaN counts as a mismatch
+}
+
+// The hopping kernels may rebuild row 2 of the SU(3) fundamental links when
+// every link passes k_check_row2 at 1e-14 (unitary links of determinant 1, up
+// to the boundary sign); otherwise they read the full links.
+static int set_recon12(int bc) {
+  L.recon12 = 0;
+  if (L.real || L.nf != 3 || L.ng != 3 || L.repr != HRGPU_FUND) return 0;
+  static int *d_bad = nullptr;
+  if (!d_bad) HR_CUDA(cudaMalloc(&d_bad, sizeof(int)));
+  HR_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), L.stream));
+  const long n = 2L * L.ld;
+  k_check_row2<<<dim3((unsigned)((n + 127) / 128), 4), 128, 0, L.stream>>>((const double2 *)L.U, make_geo(), bc,
+                                                                            1e-14, d_bad);
+  HR_LAUNCH_CHECK();
+  int bad = 1;
+  HR_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, L.stream));
+  HR_CUDA(cudaStreamSynchronize(L.stream));
+  L.recon12 = bad ? 0 : (bc ? 2 : 1);
+  return 0;
+}
+
 }  // namespace hrgpu
 
 using namespace hrgpu;
 
 extern "C" {
+
+int hrgpu_link_recon(int *mode) {
+  HR_REQUIRE(mode, HRGPU_E_ARG, "link_recon: NULL argument");
+  *mode = L.recon_allow ? L.recon12 : 0;
+  return 0;
+}
+
+int hrgpu_set_link_recon(int on) {
+  L.recon_allow = on != 0;
+  return 0;
+}
 
 int hrgpu_represent_gauge_field(int bc_t_antiperiodic) {
   HR_REQUIRE(L.ready && L.have_fund, HRGPU_E_STATE, "represent_gauge_field: no fundamental gauge field (hrgpu_gauge_set)");
@@ -139,6 +193,7 @@ int hrgpu_represent_gauge_field(int bc_t_antiperiodic) {
   HR_LAUNCH_CHECK();
   L.have_gauge = true;
   L.bc_t = bc_t_antiperiodic;
+  if (int rc = set_recon12(bc_t_antiperiodic)) return rc;
   if (int rc = hrgpu_assign_ud2u_f()) return rc;
   if (L.clover) {
     if (int rc = compute_clover_term_dev()) return rc;

@@ -186,6 +186,13 @@ class Lattice:
     def represent_gauge_field(self, bc_t_antiperiodic=True):
         _check(self.L.hrgpu_represent_gauge_field(int(bool(bc_t_antiperiodic))), "represent_gauge_field")
 
+    def link_recon(self):
+        """0: the hopping kernels read full links; 1, 2: they rebuild row 2 of the
+        SU(3) links (2: with the antiperiodic time sign)."""
+        m = ctypes.c_int(-1)
+        _check(self.L.hrgpu_link_recon(ctypes.byref(m)), "link_recon")
+        return m.value
+
     def gauge_f(self):
         dt = np.float64 if self.real else np.complex128
         uf = np.empty((self.V, 4, self.nf, self.nf), dt)

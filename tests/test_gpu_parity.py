@@ -398,3 +398,60 @@ def test_spin_structure_gamma_matrices():
             assert np.allclose(ref[mu] @ ref[nu] + ref[nu] @ ref[mu], 2.0 * eye * (mu == nu), atol=1e-15)
     prod = ref[0] @ ref[1] @ ref[2] @ ref[3]
     assert np.allclose(prod, g5, atol=1e-15) or np.allclose(prod, -g5, atol=1e-15)
+
+
+@pytest.mark.parametrize("bc", [True, False])
+def test_su3_link_reconstruction(bc):
+    """SU(3) fundamental links represented on the device pass the row-2 check,
+    and the hopping kernels then rebuild row 2 (mode 2 with the antiperiodic
+    sign, 1 without).  Wilson and clover eopre operators, FP64 and FP32, for
+    the variants that rebuild (0, 2, 5) and one that reads full links (1),
+    against the oracle and against the same links set in full
+    (hrgpu_gauge_set_f: mode 0).  A field that is not SU(3) fails the check
+    and the kernels read full links."""
+    dims = (4, 8, 8, 4)  # a time slab of 128 sites, so variant 5 applies
+    m = -0.2
+    o, lat, u, uf = setup(dims, 3, O.FUND, seed=12, smooth=0.4, bc=bc, gpu_represent=True)
+    assert lat.link_recon() == (2 if bc else 1)
+    e = F.gaussian_spinor(21, o.VH, o.nf)
+    e32 = e.astype(np.complex64)
+    fin, out = lat.field(O.EVEN, host=e), lat.field(O.EVEN)
+    f32, out32 = lat.field(O.EVEN, G.FLOAT, host=e32), lat.field(O.EVEN, G.FLOAT)
+    ref, ref32 = o.g5Dphi_eopre(m, e), o.g5Dphi_eopre_flt(m, e32)
+    try:
+        for v in (0, 1, 2, 5):
+            G._check(lat.L.hrgpu_set_hop_variant(v), "set_hop_variant")
+            lat.g5Dphi_eopre(m, out, fin)
+            assert rel(out.download(), ref) < TOL64, v
+            lat.g5Dphi_eopre_flt(m, out32, f32)
+            assert rel(out32.download(), ref32) < 10 * TOL32, v
+        G._check(lat.L.hrgpu_set_hop_variant(0), "set_hop_variant")
+        lat.g5Dphi_eopre(m, out, fin)
+        rebuilt = out.download()
+        lat.clover_init(1.0)
+        o.clover_init(1.0)
+        o.compute_clover_term()
+        lat.g5Cphi_eopre(m, out, fin)
+        assert rel(out.download(), o.g5Cphi_eopre(m, e)) < TOL64
+    finally:
+        G._check(lat.L.hrgpu_set_hop_variant(-1), "set_hop_variant")
+    # the same links set in full: the kernels read all three rows
+    lat2 = G.Lattice(*dims, 3, G.FUND, ipt=o.geometry()[0])
+    lat2.set_gauge_f(uf)
+    assert lat2.link_recon() == 0
+    out2 = lat2.field(O.EVEN)
+    lat2.g5Dphi_eopre(m, out2, lat2.field(O.EVEN, host=e))
+    assert rel(rebuilt, out2.download()) < 1e-14
+    # links that are not SU(3): no reconstruction, and still the oracle's operator
+    ub = u * 1.05
+    o.set_gauge(o.represent_gauge_field(ub, bc))
+    o.clover_init(1.0)
+    o.compute_clover_term()
+    lat3 = G.Lattice(*dims, 3, G.FUND, ipt=o.geometry()[0])
+    lat3.set_gauge(ub)
+    lat3.represent_gauge_field(bc)
+    assert lat3.link_recon() == 0
+    lat3.clover_init(1.0)
+    out3 = lat3.field(O.EVEN)
+    lat3.g5Cphi_eopre(m, out3, lat3.field(O.EVEN, host=e))
+    assert rel(out3.download(), o.g5Cphi_eopre(m, e)) < TOL64
