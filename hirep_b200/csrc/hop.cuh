@@ -142,9 +142,29 @@ __device__ __forceinline__ void link_mul(float2 *chi, const float2 *h, const __n
 // kernels instantiated for reconstruction): only rows 0 and 1 are loaded and
 // row 2 is rebuilt as sg conj(r0 x r1) (su3_row2), a third less link traffic;
 // otherwise the full link is read.
-template <int NA, bool DAG, bool R12, typename V, typename E, typename R>
+// The real form (R12R: SU(2) adjoint links, SO(3)) rebuilds row 2 as sg (r0 x r1).
+template <int NA, bool DAG, bool R12, bool R12R = false, typename V, typename E, typename R>
 __device__ __forceinline__ void link_mul2(V *c0, V *c1, const V *h0, const V *h1, const E *U, long plane, long site,
                                           int nf, R sg) {
+  if constexpr (R12R) {
+    R u[9];
+#pragma unroll
+    for (int e = 0; e < 6; e++) u[e] = ld_c(U + (long)e * plane + site);
+    so3_row2(u, sg);
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      V a0 = cmk<V>(0.0, 0.0), a1 = cmk<V>(0.0, 0.0);
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        const R w = DAG ? u[3 * j + i] : u[3 * i + j];
+        rmac(a0, w, h0[j]);
+        rmac(a1, w, h1[j]);
+      }
+      c0[i] = a0;
+      c1[i] = a1;
+    }
+    return;
+  }
   if constexpr (R12) {
     {
       V u[9];
@@ -293,6 +313,7 @@ __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb, co
   typedef LE E;
   constexpr int NA = NFT;
   constexpr bool R12 = RC && NFT == 3 && !REAL && std::is_same<LE, V>::value;
+  constexpr bool R12R = RC && NFT == 3 && REAL && std::is_same<LE, R>::value;
   const int nf = NFT;
   const Geo g = a.g;
   double nrm = 0.0;
@@ -335,7 +356,7 @@ __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb, co
           if (mu == 3) { h0[i] = caddi(s0, s2); h1[i] = csubi(s1, s3); }
         }
         const R sgf = (a.recon == 2 && mu == 0 && t == 0) ? (R)-1 : (R)1;
-        link_mul2<NA, false, R12>(c0, c1, h0, h1, Umu, lplane, so, nf, sgf);
+        link_mul2<NA, false, R12, R12R>(c0, c1, h0, h1, Umu, lplane, so, nf, sgf);
 #pragma unroll
         for (int i = 0; i < NA; i++) {
           if (i >= nf) break;
@@ -363,7 +384,7 @@ __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb, co
         }
         const long sn = (long)inp * g.ld + cdn;
         const R sgb = (a.recon == 2 && mu == 0 && tm == 0) ? (R)-1 : (R)1;
-        link_mul2<NA, true, R12>(c0, c1, h0, h1, Umu, lplane, sn, nf, sgb);
+        link_mul2<NA, true, R12, R12R>(c0, c1, h0, h1, Umu, lplane, sn, nf, sgb);
 #pragma unroll
         for (int i = 0; i < NA; i++) {
           if (i >= nf) break;
@@ -432,7 +453,7 @@ __device__ __forceinline__ void pdl_enter() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
-// RC: rebuild row 2 of the SU(3) links (instantiated for complex NF = 3 only)
+// RC: rebuild row 2 of the 3x3 links (instantiated for NF = 3 only)
 template <int NFT, bool REAL, typename R, int EP, int MINB, typename LE = typename LinkE<REAL, R>::T, bool RC = false>
 __global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop(HopArgs<R> a) {
   pdl_enter();

@@ -69,10 +69,11 @@ int launch_tma(HopArgs<R> &a, dim3 grid, dim3 block, cudaStream_t s) {
 }
 
 // k_hop for variants 0 and 2: the instantiation that rebuilds row 2 of the
-// SU(3) links when the links passed the check, else the one reading full links
+// 3x3 links (SU(3) fundamental, SU(2) adjoint) when the links passed the
+// check, else the one reading full links
 template <int N, bool RL, typename R, int EP, int MINB>
 static inline void (*hop_kernel(int recon))(HopArgs<R>) {
-  if constexpr (N == 3 && !RL) {
+  if constexpr (N == 3) {
     if (recon) return k_hop<N, RL, R, EP, MINB, typename LinkE<RL, R>::T, true>;
   }
   return k_hop<N, RL, R, EP, MINB>;

@@ -85,9 +85,10 @@ struct Lattice {
   double *force_sum = nullptr;    // [4][dimg][2*ld]
   double *mom = nullptr;          // momenta [4][dimg][2*ld]
   int bc_t = 1;                   // time boundary condition of the last represent_gauge_field
-  // hopping kernels rebuild row 2 of each SU(3) link from rows 0 and 1: 0 no
-  // (full loads), 1 yes, 2 yes with the antiperiodic-T sign on mu = 0 links at
-  // t = 0 (set by represent_gauge_field after checking every link)
+  // hopping kernels rebuild row 2 of each 3x3 link (SU(3) fundamental, SU(2)
+  // adjoint) from rows 0 and 1: 0 no (full loads), 1 yes, 2 yes with the
+  // antiperiodic-T sign on mu = 0 links at t = 0 (set by represent_gauge_field
+  // after checking every link)
   int recon12 = 0;
   bool recon_allow = true;        // hrgpu_set_link_recon
   double2 *cl_force = nullptr;    // [6][nf*nf][2*ld]
@@ -183,6 +184,15 @@ template <typename V> __device__ __forceinline__ V cmul(V a, V b) {
 // u[0..5], row-major): u[6..8] = s conj(r0 x r1).  For U in SU(3) (s = 1), and
 // for -U (s = -1, a link that carries the antiperiodic time sign), this is the
 // stored row to rounding.
+// the same for a real orthogonal 3x3 link (SU(2) in the adjoint
+// representation, SO(3)): u[6..8] = s (r0 x r1)
+template <typename R>
+__device__ __forceinline__ void so3_row2(R *u, R s) {
+  u[6] = s * (u[1] * u[5] - u[2] * u[4]);
+  u[7] = s * (u[2] * u[3] - u[0] * u[5]);
+  u[8] = s * (u[0] * u[4] - u[1] * u[3]);
+}
+
 template <typename V, typename R>
 __device__ __forceinline__ void su3_row2(V *u, R s) {
   V q;

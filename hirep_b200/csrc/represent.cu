@@ -144,18 +144,42 @@ __global__ void k_check_row2(const double2 *U, Geo g, int bc, double tol, int *b
   if (!(dev <= tol)) atomicOr(bad, 1);  // NaN counts as a mismatch
 }
 
-// The hopping kernels may rebuild row 2 of the SU(3) fundamental links when
-// every link passes k_check_row2 at 1e-14 (unitary links of determinant 1, up
-// to the boundary sign); otherwise they read the full links.
+// the same for real links (SU(2) adjoint): row 2 against s (r0 x r1)
+__global__ void k_check_row2_real(const double *U, Geo g, int bc, double tol, int *bad) {
+  const long d = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int mu = blockIdx.y;
+  if (d >= 2L * g.ld) return;
+  const int p = d >= g.ld ? 1 : 0, cb = (int)(d - (long)p * g.ld);
+  if (cb >= g.VH) return;
+  int t, x, y, z;
+  cb_to_coords(g, cb, p, t, x, y, z);
+  const long plane = 2L * g.ld;
+  const double *Um = U + (long)mu * 9 * plane + d;
+  double u[9];
+  for (int e = 0; e < 9; e++) u[e] = Um[(long)e * plane];
+  const double r6 = u[6], r7 = u[7], r8 = u[8];
+  so3_row2(u, (bc && mu == 0 && t == 0) ? -1.0 : 1.0);
+  const double dev = fmax(fabs(u[6] - r6), fmax(fabs(u[7] - r7), fabs(u[8] - r8)));
+  if (!(dev <= tol)) atomicOr(bad, 1);  // NaN counts as a mismatch
+}
+
+// The hopping kernels may rebuild row 2 of the SU(3) fundamental or SU(2)
+// adjoint links when every link passes the check at 1e-14 (unitary links of
+// determinant 1, up to the boundary sign); otherwise they read the full links.
 static int set_recon12(int bc) {
   L.recon12 = 0;
-  if (L.real || L.nf != 3 || L.ng != 3 || L.repr != HRGPU_FUND) return 0;
+  const bool su3 = !L.real && L.nf == 3 && L.ng == 3 && L.repr == HRGPU_FUND;
+  const bool so3 = L.real && L.nf == 3 && L.ng == 2 && L.repr == HRGPU_ADJ;
+  if (!su3 && !so3) return 0;
   static int *d_bad = nullptr;
   if (!d_bad) HR_CUDA(cudaMalloc(&d_bad, sizeof(int)));
   HR_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), L.stream));
   const long n = 2L * L.ld;
-  k_check_row2<<<dim3((unsigned)((n + 127) / 128), 4), 128, 0, L.stream>>>((const double2 *)L.U, make_geo(), bc,
-                                                                            1e-14, d_bad);
+  const dim3 grid((unsigned)((n + 127) / 128), 4);
+  if (su3)
+    k_check_row2<<<grid, 128, 0, L.stream>>>((const double2 *)L.U, make_geo(), bc, 1e-14, d_bad);
+  else
+    k_check_row2_real<<<grid, 128, 0, L.stream>>>((const double *)L.U, make_geo(), bc, 1e-14, d_bad);
   HR_LAUNCH_CHECK();
   int bad = 1;
   HR_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, L.stream));

@@ -91,10 +91,10 @@ int hrgpu_gauge_set(const double *u_host);
  * the antiperiodic-T link sign (LibHR/Utils/boundary_conditions.c:321-341) and,
  * with a clover term, compute_clover_term; also refreshes the float copy (assign_ud2u_f) */
 int hrgpu_represent_gauge_field(int bc_t_antiperiodic);
-/* SU(3) fundamental links: after represent_gauge_field has checked that every
- * link's row 2 equals s conj(r0 x r1) to 1e-14 (s = -1 on the links with the
- * antiperiodic time sign), the single-field hopping kernels load rows 0 and 1
- * only and rebuild row 2.  mode: 0 full links (any other group or
+/* SU(3) fundamental and SU(2) adjoint links: after represent_gauge_field has
+ * checked that every link's row 2 equals s conj(r0 x r1) (adjoint: s (r0 x r1))
+ * to 1e-14 (s = -1 on the links with the antiperiodic time sign), the
+ * single-field hopping kernels load rows 0 and 1 only and rebuild row 2.  mode: 0 full links (any other group or
  * representation, a field that fails the check, links set with
  * hrgpu_gauge_set_f), 1 rebuilt, 2 rebuilt with the antiperiodic sign.  No
  * counterpart in the reference, which reads the full links. */

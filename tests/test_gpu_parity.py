@@ -400,18 +400,18 @@ def test_spin_structure_gamma_matrices():
     assert np.allclose(prod, g5, atol=1e-15) or np.allclose(prod, -g5, atol=1e-15)
 
 
+@pytest.mark.parametrize("ng,rep", [(3, O.FUND), (2, O.ADJ)])
 @pytest.mark.parametrize("bc", [True, False])
-def test_su3_link_reconstruction(bc):
-    """SU(3) fundamental links represented on the device pass the row-2 check,
-    and the hopping kernels then rebuild row 2 (mode 2 with the antiperiodic
-    sign, 1 without).  Wilson and clover eopre operators, FP64 and FP32, for
-    the variants that rebuild (0, 2, 5) and one that reads full links (1),
-    against the oracle and against the same links set in full
-    (hrgpu_gauge_set_f: mode 0).  A field that is not SU(3) fails the check
-    and the kernels read full links."""
+def test_link_reconstruction(ng, rep, bc):
+    """SU(3) fundamental and SU(2) adjoint links represented on the device pass
+    the row-2 check, and the hopping kernels then rebuild row 2 (mode 2 with
+    the antiperiodic sign, 1 without).  Wilson and clover eopre operators, FP64
+    and FP32, for the variants 0-2 and 5 (0 and 2 rebuild), against the oracle
+    and against the same links set in full (hrgpu_gauge_set_f: mode 0).  A
+    field that is not unitary fails the check and the kernels read full links."""
     dims = (4, 8, 8, 4)  # a time slab of 128 sites, so variant 5 applies
     m = -0.2
-    o, lat, u, uf = setup(dims, 3, O.FUND, seed=12, smooth=0.4, bc=bc, gpu_represent=True)
+    o, lat, u, uf = setup(dims, ng, rep, seed=12, smooth=0.4, bc=bc, gpu_represent=True)
     assert lat.link_recon() == (2 if bc else 1)
     e = F.gaussian_spinor(21, o.VH, o.nf)
     e32 = e.astype(np.complex64)
@@ -436,7 +436,7 @@ def test_su3_link_reconstruction(bc):
     finally:
         G._check(lat.L.hrgpu_set_hop_variant(-1), "set_hop_variant")
     # the same links set in full: the kernels read all three rows
-    lat2 = G.Lattice(*dims, 3, G.FUND, ipt=o.geometry()[0])
+    lat2 = G.Lattice(*dims, ng, rep, ipt=o.geometry()[0])
     lat2.set_gauge_f(uf)
     assert lat2.link_recon() == 0
     out2 = lat2.field(O.EVEN)
@@ -447,7 +447,7 @@ def test_su3_link_reconstruction(bc):
     o.set_gauge(o.represent_gauge_field(ub, bc))
     o.clover_init(1.0)
     o.compute_clover_term()
-    lat3 = G.Lattice(*dims, 3, G.FUND, ipt=o.geometry()[0])
+    lat3 = G.Lattice(*dims, ng, rep, ipt=o.geometry()[0])
     lat3.set_gauge(ub)
     lat3.represent_gauge_field(bc)
     assert lat3.link_recon() == 0
