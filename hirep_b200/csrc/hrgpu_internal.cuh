@@ -138,6 +138,7 @@ inline size_t spinor_bytes(int par, int prec) {
 
 int ensure_tmp(void **p, size_t bytes);
 int ensure_links_bf16();  // the BF16 copy of the links, made from the FP64 ones when they changed
+int detect_recon12();     // check links set already represented for row-2 reconstruction
 int compute_clover_term_dev();
 void cg_release();
 int ensure_stage(size_t bytes);

@@ -560,7 +560,7 @@ int hrgpu_gauge_set_f(const void *uf_host) {
   HR_CUDA(cudaMemcpyAsync(L.stage, uf_host, bytes, cudaMemcpyHostToDevice, L.stream));
   if (int rc = launch_links_in(L.U, L.stage, nel, L.real, 4)) return rc;
   L.have_gauge = true;
-  L.recon12 = 0;  // links set directly: the hopping kernels read them in full
+  if (int rc = detect_recon12()) return rc;
   if (int rc = hrgpu_assign_ud2u_f()) return rc;
   if (L.clover) {
     if (int rc = compute_clover_term_dev()) return rc;

@@ -188,6 +188,15 @@ static int set_recon12(int bc) {
   return 0;
 }
 
+// links uploaded already represented (hrgpu_gauge_set_f): the boundary
+// condition is not known, so try the antiperiodic sign, then none
+int detect_recon12() {
+  if (int rc = set_recon12(1)) return rc;
+  if (L.recon12 == 0)
+    if (int rc = set_recon12(0)) return rc;
+  return 0;
+}
+
 }  // namespace hrgpu
 
 using namespace hrgpu;

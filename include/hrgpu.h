@@ -94,10 +94,11 @@ int hrgpu_represent_gauge_field(int bc_t_antiperiodic);
 /* SU(3) fundamental and SU(2) adjoint links: after represent_gauge_field has
  * checked that every link's row 2 equals s conj(r0 x r1) (adjoint: s (r0 x r1))
  * to 1e-14 (s = -1 on the links with the antiperiodic time sign), the
- * single-field hopping kernels load rows 0 and 1 only and rebuild row 2.  mode: 0 full links (any other group or
- * representation, a field that fails the check, links set with
- * hrgpu_gauge_set_f), 1 rebuilt, 2 rebuilt with the antiperiodic sign.  No
- * counterpart in the reference, which reads the full links. */
+ * single-field hopping kernels load rows 0 and 1 only and rebuild row 2.
+ * hrgpu_gauge_set_f runs the same check, trying the antiperiodic sign first.
+ * mode: 0 full links (any other group or representation, a field that fails
+ * the check), 1 rebuilt, 2 rebuilt with the antiperiodic sign.  No counterpart
+ * in the reference, which reads the full links. */
 int hrgpu_link_recon(int *mode);
 /* allow (1, default) or forbid (0) the row-2 reconstruction above */
 int hrgpu_set_link_recon(int on);

@@ -405,10 +405,11 @@ def test_spin_structure_gamma_matrices():
 def test_link_reconstruction(ng, rep, bc):
     """SU(3) fundamental and SU(2) adjoint links represented on the device pass
     the row-2 check, and the hopping kernels then rebuild row 2 (mode 2 with
-    the antiperiodic sign, 1 without).  Wilson and clover eopre operators, FP64
-    and FP32, for the variants 0-2 and 5 (0 and 2 rebuild), against the oracle
-    and against the same links set in full (hrgpu_gauge_set_f: mode 0).  A
-    field that is not unitary fails the check and the kernels read full links."""
+    the antiperiodic sign, 1 without); links uploaded already represented
+    (hrgpu_gauge_set_f) are checked the same way.  Wilson and clover eopre
+    operators, FP64 and FP32, for the variants 0-2 and 5 (0 and 2 rebuild),
+    against the oracle and against the full-link kernels.  A field that is not
+    unitary fails the check and the kernels read full links."""
     dims = (4, 8, 8, 4)  # a time slab of 128 sites, so variant 5 applies
     m = -0.2
     o, lat, u, uf = setup(dims, ng, rep, seed=12, smooth=0.4, bc=bc, gpu_represent=True)
@@ -435,12 +436,18 @@ def test_link_reconstruction(ng, rep, bc):
         assert rel(out.download(), o.g5Cphi_eopre(m, e)) < TOL64
     finally:
         G._check(lat.L.hrgpu_set_hop_variant(-1), "set_hop_variant")
-    # the same links set in full: the kernels read all three rows
+    # the same links uploaded already represented: the check finds the mode
+    # again; with reconstruction forbidden the kernels read all three rows
     lat2 = G.Lattice(*dims, ng, rep, ipt=o.geometry()[0])
     lat2.set_gauge_f(uf)
-    assert lat2.link_recon() == 0
+    assert lat2.link_recon() == (2 if bc else 1)
     out2 = lat2.field(O.EVEN)
-    lat2.g5Dphi_eopre(m, out2, lat2.field(O.EVEN, host=e))
+    try:
+        G._check(lat2.L.hrgpu_set_link_recon(0), "set_link_recon")
+        assert lat2.link_recon() == 0
+        lat2.g5Dphi_eopre(m, out2, lat2.field(O.EVEN, host=e))
+    finally:
+        G._check(lat2.L.hrgpu_set_link_recon(1), "set_link_recon")
     assert rel(rebuilt, out2.download()) < 1e-14
     # links that are not SU(3): no reconstruction, and still the oracle's operator
     ub = u * 1.05
