@@ -18,8 +18,10 @@
 //
 // In host code the array's name is only a host-side stand-in, so its device
 // address is looked up with cudaGetSymbolAddress once per device, with that
-// device current, by the first call made on that device.  Make that first call
-// before any stream capture.
+// device current, by the first call made on that device.  If no FP64 operator
+// has run on the lattice yet, that first call also times the hopping-kernel
+// variants (two CUDA events and a synchronisation, no device memory).  Make
+// that first call before any stream capture.
 //
 // All calls share the one array and it keeps whatever the last call left
 // there.  Nothing in it has to start at zero: the first hop writes every site
