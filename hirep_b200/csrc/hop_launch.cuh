@@ -223,6 +223,13 @@ int launch_ep(HopArgs<R> &a) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (trc) return trc;
+    // the candidates are timed on back-to-back launches with the operands
+    // warm in L2, which favours the register-capped variants slightly over a
+    // cold step (16^3x32 FP64: variant 2 1.5 % ahead warm, variant 0 1.5 %
+    // ahead with L2 flushed): another variant replaces variant 0 only when it
+    // is at least 3 % faster
+    const float t0 = L.hop_tune_ms[pi][EP][0];
+    if (bestv != 0 && t0 > 0.0f && best / 3.0f > 0.97f * t0) bestv = 0;
     v = bestv;
   }
   int rc = launch_ep_variant<R, EP>(a, v);
