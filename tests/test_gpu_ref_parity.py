@@ -1,0 +1,195 @@
+"""The CUDA path against HiRep itself: the golden fixtures written by HiRep
+(tests/golden/make_golden.py) and the reference's own library run live through
+oracle/_ref/<config>/hr_ref (built from the reference sources by
+oracle/ref/Makefile; the executables travel with the repository, nothing reads
+the reference sources at run time).
+
+Small lattices: every fixture field (even-odd operator, CG solution and MVM
+count, force).  Full sizes: config 1 on HiRep's own hot start (ranlux seed
+1234) and Gaussian source, config 2's Cphi_eopre, config 3's force, config 4's
+sextet clover Cphi_eopre and config 5's adjoint Dphi_eopre, each against
+HiRep's output for the same fields.  HiRep's clover builds run with one
+OpenMP thread (its Cphi_ shares its temporaries between threads,
+LibHR/Update/Dphi.c:1092-1146).
+
+Tolerances: FP64 fields 1e-13 relative (max-norm) for operators, 1e-12 for
+CG solutions and forces; MVM counts within 3 of HiRep's (the CG takes alpha
+from |Hk|^2 and sums in a fixed device order, so the last iterations can
+differ at rounding level).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import hirep_ref as H
+import oracle as O
+from hirep_b200 import fields as F
+from hirep_b200 import hrgpu as G
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+REP = {"FUND": G.FUND, "ADJ": G.ADJ, "SYM": G.SYM, "ASYM": G.ASYM}
+FIXTURES = ["su3_fund", "su3_fund_clover", "su4_asym", "su2_adj", "su3_sym_clover"]
+MASS, CSW, DT, RES = -0.1, 1.0, 0.37, 1.3
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+def need(cfg):
+    if not H.available(cfg):
+        pytest.skip(f"HiRep build {cfg} not present (make -C oracle/ref)")
+
+
+def lattice(dims, cfg, u, bc=True, clover=None):
+    ng, rep, _ = H.CONFIGS[cfg]
+    lat = G.Lattice(*dims, ng, REP[rep], ipt=G.geometry(*dims)[0])
+    lat.set_gauge(u)
+    lat.represent_gauge_field(bc)
+    if clover is not None:
+        lat.clover_init(clover)
+    return lat
+
+
+def force_of(lat, X, Y, m, dt, res):
+    lat.set_dirac_mass(m)
+    lat.fermion_force_begin()
+    lat.force_fermion_core(lat.field(G.FULL, host=X), lat.field(G.FULL, host=Y), 1, dt, res)
+    return lat.fermion_force_end(dt, np.zeros((lat.V, 4, lat.ng * lat.ng - 1)))
+
+
+@pytest.mark.parametrize("cfg", FIXTURES)
+def test_gpu_matches_hirep_fixture(cfg):
+    ng, _, clover = H.CONFIGS[cfg]
+    g = np.load(os.path.join(GOLDEN, f"hirep_{cfg}.npz"))
+    dims = (4, 4, 4, 4)
+    V = 256
+    lat = lattice(dims, cfg, F.smooth_gauge(7, V, ng, 0.3), clover=CSW if clover else None)
+    nf = lat.nf
+    e = F.gaussian_spinor(1, V // 2, nf)
+    fe, out = lat.field(G.EVEN, host=e), lat.field(G.EVEN)
+    (lat.Cphi_eopre if clover else lat.Dphi_eopre)(MASS, out, fe)
+    assert rel(out.download(), g["eopre"]) < 1e-13
+    x = lat.field(G.EVEN)
+    op = G.OP_G5CPHI_EOPRE_SQ if clover else G.OP_G5DPHI_EOPRE_SQ
+    it, ok = lat.cg_mshift(op, MASS, [0.1], 1e-28, fe, [x], max_iter=5000)
+    assert ok
+    assert abs(it - int(g["cg_mvm"])) <= 3
+    assert rel(x.download(), g["cg"][0]) < 1e-12
+    f = force_of(lat, F.gaussian_spinor(11, V, nf), F.gaussian_spinor(12, V, nf), MASS, DT, RES)
+    assert rel(f, g["force"]) < 1e-12
+
+
+def test_gpu_geometry_matches_hirep_fixture():
+    g = np.load(os.path.join(GOLDEN, "hirep_geometry_4x6x2x8.npz"))
+    ipt, iup, idn = G.geometry(4, 6, 2, 8)
+    assert np.array_equal(ipt, g["ipt"]) and np.array_equal(iup, g["iup"]) and np.array_equal(idn, g["idn"])
+
+
+def test_config1_on_hireps_hot_start():
+    """Config 1 as specified: SU(3) fundamental 8^4, HiRep's random_u after
+    rlxd_init(1, 1234), a unit-variance Gaussian source from HiRep's ranlux
+    (gaussian_spinor_field has variance 1/2 per component, random_spinor_field.c:14-24,
+    so it is scaled by sqrt 2); Dphi and Dphi_eopre at m0 = 0.1 and CG on
+    g5Dphi_sq to |r|/|b| < 1e-14, against HiRep's own results."""
+    need("su3_fund")
+    dims, m = (8, 8, 8, 8), 0.1
+    with H.HiRep("su3_fund", *dims, seed=1234) as h:
+        u = h.random_u()
+        src = h.gaussian_spinor_field(H.FULL) * np.sqrt(2.0)
+        e = src[: h.VH].copy()
+        d_h = h.Dphi(m, src)
+        eo_h = h.Dphi_eopre(m, e)
+        x_h, mvm_h = h.cg_mshift("g5Dphi_sq", m, [0.0], 1e-28, src, H.FULL, max_iter=5000)
+        plaq = h.plaquette()
+    g = np.load(os.path.join(GOLDEN, "hirep_config1.npz"))
+    assert abs(plaq - float(g["plaquette"])) < 1e-14  # the build reproduces the fixture's ranlux stream
+    # u_gauge read back already carries the antiperiodic sign (fundamental: u_gauge_f is u_gauge)
+    lat = lattice(dims, "su3_fund", u, bc=False)
+    fs, out = lat.field(G.FULL, host=src), lat.field(G.FULL)
+    lat.Dphi(m, out, fs)
+    assert rel(out.download(), d_h) < 1e-13
+    fe, oe = lat.field(G.EVEN, host=e), lat.field(G.EVEN)
+    lat.Dphi_eopre(m, oe, fe)
+    assert rel(oe.download(), eo_h) < 1e-13
+    x = lat.field(G.FULL)
+    it, ok = lat.cg_mshift(G.OP_G5DPHI_SQ, m, [0.0], 1e-28, fs, [x], max_iter=5000)
+    assert ok
+    assert abs(it - mvm_h) <= 3
+    assert rel(x.download(), x_h[0]) < 1e-12
+
+
+def test_config2_full_size_cphi_eopre_is_hireps():
+    """SU(3) fundamental, clover csw = 1.0, m0 = -0.2, 16^3 x 32, U = exp(i 0.3 H)
+    seed 7: Cphi_eopre and g5Cphi_eopre_sq against HiRep's at the full size."""
+    need("su3_fund_clover")
+    dims, m = (32, 16, 16, 16), -0.2
+    u = F.smooth_gauge(7, 32 * 16 ** 3, 3, 0.3)
+    e = F.gaussian_spinor(1, 16 ** 4, 3)
+    with H.HiRep("su3_fund_clover", *dims, threads=1) as h:
+        h.set_gauge(u)
+        h.set_csw(1.0)
+        want = h.Cphi_eopre(m, e)
+        want_sq = h.g5Cphi_eopre_sq(m, e)
+    lat = lattice(dims, "su3_fund_clover", u, clover=1.0)
+    fe, out = lat.field(G.EVEN, host=e), lat.field(G.EVEN)
+    lat.Cphi_eopre(m, out, fe)
+    assert rel(out.download(), want) < 1e-13
+    lat.g5Cphi_eopre_sq(m, out, fe)
+    assert rel(out.download(), want_sq) < 1e-13
+    # the host-field (e2e) path gives the same field
+    assert rel(lat.apply_op_host(G.OP_CPHI_EOPRE, m, e), want) < 1e-13
+
+
+def test_config3_full_size_force_is_hireps():
+    """SU(4) two-index antisymmetric (NF = 6), Wilson m0 = -0.1, 16^4, links
+    exp(i 0.25 H) seed 11: force_fermion_core (odd-site fill included) +
+    fermion_force_end against HiRep's at the full size."""
+    need("su4_asym")
+    dims, m = (16, 16, 16, 16), -0.1
+    u = F.smooth_gauge(11, 16 ** 4, 4, 0.25)
+    X = F.gaussian_spinor(31, 16 ** 4, 6)
+    Y = F.gaussian_spinor(32, 16 ** 4, 6)
+    with H.HiRep("su4_asym", *dims) as h:
+        h.set_gauge(u)
+        want = h.force(m, 0.3, 1.0, X, Y, True)
+    lat = lattice(dims, "su4_asym", u)
+    assert rel(force_of(lat, X, Y, m, 0.3, 1.0), want) < 1e-12
+
+
+def test_config4_full_size_sextet_clover_is_hireps():
+    """SU(3) two-index symmetric (NF = 6), clover csw = 1.0, m0 = -0.3, 24^3 x 48,
+    links exp(i 0.3 H) seed 21: the single-field Cphi_eopre against HiRep's."""
+    need("su3_sym_clover")
+    dims, m = (48, 24, 24, 24), -0.3
+    V = 48 * 24 ** 3
+    u = F.smooth_gauge(21, V, 3, 0.3)
+    e = F.gaussian_spinor(2, V // 2, 6)
+    with H.HiRep("su3_sym_clover", *dims, threads=1) as h:
+        h.set_gauge(u)
+        h.set_csw(1.0)
+        want = h.Cphi_eopre(m, e)
+    lat = lattice(dims, "su3_sym_clover", u, clover=1.0)
+    fe, out = lat.field(G.EVEN, host=e), lat.field(G.EVEN)
+    lat.Cphi_eopre(m, out, fe)
+    assert rel(out.download(), want) < 1e-13
+
+
+def test_config5_full_size_adjoint_is_hireps():
+    """SU(2) adjoint (NF = 3, real links), Wilson m0 = -1.0, 32^3 x 64, links
+    exp(i 0.2 H) seed 99: Dphi_eopre against HiRep's at the full size."""
+    need("su2_adj")
+    dims, m = (64, 32, 32, 32), -1.0
+    V = 64 * 32 ** 3
+    u = F.smooth_gauge(99, V, 2, 0.2)
+    e = F.gaussian_spinor(5, V // 2, 3)
+    with H.HiRep("su2_adj", *dims) as h:
+        h.set_gauge(u)
+        want = h.Dphi_eopre(m, e)
+    lat = lattice(dims, "su2_adj", u)
+    fe, out = lat.field(G.EVEN, host=e), lat.field(G.EVEN)
+    lat.Dphi_eopre(m, out, fe)
+    assert rel(out.download(), want) < 1e-13
