@@ -11,19 +11,28 @@ kernel.  value = GB/s under HiRep's own byte model
 (TestProgram/DiracOperator/speed_test_diracoperator.c:77-82: 36 vectors + 8
 links per site and hop) plus the clover blocks and the (4+m)^2 input read:
     V * 2880 + V/2 * 192 + V/2 * (672 + 576) bytes per application.
-Each application touches about 190 MB, but one launch only about 130 MB,
-close to the 126 MB L2, so L2 is flushed between timed steps: a 512 MB buffer
-is written and then another 512 MB buffer is read, which leaves L2 holding
-clean lines of unrelated data.  Times are CUDA events on the library's stream.
+The roofline fraction is taken on the bytes the kernels must move at least
+(every link once per hop, read as two rows where the links are rebuilt, the
+fields in and out, the packed clover blocks once), not on HiRep's model, which
+counts each neighbour spinor eight times.  Each application touches about 240
+MB, one launch about 130 MB, close to the 126 MB L2, so L2 is flushed between
+timed steps: a 512 MB buffer is written and then another 512 MB buffer is read,
+which leaves L2 holding clean lines of unrelated data.  Times are CUDA events
+on the library's stream.
 
 Besides the step the run reports the time to |r|/|b| < 1e-12 (err2 = 1e-24) of
 the plain FP64 CG and of the FP32-inner defect-correction CG on g5Cphi_eopre^2,
 the end-to-end rate through the C ABI with host buffers, the roofline of the
-hopping kernel against the measured HBM copy bandwidth, and the CPU oracle on
-the host cores as a reported baseline.
+hopping kernel against the measured HBM copy bandwidth, the single-field
+even-odd operator of the other workloads (16^4 SU(4) antisymmetric, 24^3x48
+sextet clover, 32^3x64 SU(2) adjoint) with their rooflines, and HiRep's own
+OpenMP build on the host cores as a reported baseline.
 
---impl reference times the CPU restatement of HiRep's operator (the reference
-itself needs generated headers and is not built here) on all host cores.
+--impl reference times HiRep itself: the reference's library built from its
+sources (oracle/ref/Makefile into oracle/_ref/), its Cphi_eopre on the same
+fields, on all host cores (OMP_PROC_BIND=close), median of the timed
+applications as TestProgram/DiracOperator/speed_test_diracoperator.c times
+its operator.
 With --gpus N (torchrun) every rank runs an independent replica on its own GPU
 (the single-GPU scope has no halo exchange); value is the sum over ranks and
 the time the max over ranks.
@@ -51,6 +60,19 @@ METRIC = "eopre Dslash GB/s (%HBM peak); time to |r|/|b|<1e-12, mixed vs FP64 so
 
 def eopre_bytes(V):
     return V * SITE_BYTES + (V // 2) * SPINOR_BYTES + (V // 2) * CLOVER_BYTES
+
+
+def unique_bytes(V, nf, real, link_rows, clover):
+    """Bytes one FP64 even-odd application must move at least: every link once
+    per hop (link_rows of its NF rows, real or complex), the even input twice
+    (hop 1 and the diagonal term of hop 2), the odd temporary written and read,
+    the even output written, and the packed clover blocks (D^-1 on the odd
+    sites, D on the even ones) once."""
+    esz = 8 if real else 16
+    links = 2 * 4 * V * link_rows * nf * esz
+    spinors = 5 * (V // 2) * 4 * nf * 16
+    blocks = V * (2 * 2 * nf * 8 + 2 * nf * (2 * nf - 1) * 16) if clover else 0
+    return links + spinors + blocks
 
 
 def workload_config():
@@ -133,8 +155,8 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def cpu_reference_arm(args):
-    """The CPU restatement of HiRep's operator on all host cores (reference arm / cpu_baseline)."""
+def cpu_port_arm(seconds):
+    """The CPU restatement of HiRep's operator (oracle/hr_oracle.c) on all host cores."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     from hirep_b200 import fields as F
@@ -148,15 +170,47 @@ def cpu_reference_arm(args):
     src = F.gaussian_spinor(SEED, o.VH, o.nf)
     o.Cphi_eopre(MASS, src)  # builds the LDL cache
     times = []
-    t_end = time.perf_counter() + args.cpu_seconds
+    t_end = time.perf_counter() + seconds
     while len(times) < 3 or (time.perf_counter() < t_end and len(times) < 200):
         t0 = time.perf_counter()
         o.Cphi_eopre(MASS, src)
         times.append(time.perf_counter() - t0)
     t = float(np.median(times))
-    gbs = eopre_bytes(o.V) / t / 1e9
-    return {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
-            "sample": f"{len(times)} Cphi_eopre applications on 16^3x32 (median {t * 1e3:.1f} ms), OpenMP"}, t
+    return {"value": eopre_bytes(o.V) / t / 1e9, "unit": "GB/s", "cores": threads, "kind": "port",
+            "sample": f"{len(times)} Cphi_eopre applications on 16^3x32 (median {t * 1e3:.1f} ms), OpenMP"}
+
+
+def cpu_reference_arm(args):
+    """HiRep's own Cphi_eopre (LibHR/Update/Dphi.c:1240-1255) from the reference's
+    library built from its sources, on all host cores, timed as its speed test
+    times its operator (warm-up, then the median of >= 20 applications).  Falls
+    back to the CPU restatement where the HiRep build is absent."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import hirep_ref as H
+    from hirep_b200 import fields as F
+
+    if not H.available("su3_fund_clover"):
+        base = cpu_port_arm(args.cpu_seconds)
+        return base, eopre_bytes(DIMS[0] * DIMS[1] * DIMS[2] * DIMS[3]) / base["value"] / 1e9
+    threads = os.cpu_count() or 1
+    V = DIMS[0] * DIMS[1] * DIMS[2] * DIMS[3]
+    u = F.smooth_gauge(SEED, V, NG, EPS)
+    src = F.gaussian_spinor(SEED, V // 2, 3)
+    with H.HiRep("su3_fund_clover", *DIMS, threads=threads) as h:
+        h.set_gauge(u)
+        h.set_csw(CSW)
+        # one probe decides the count: 20..200 applications, about args.cpu_seconds
+        probe, _, _ = h.time_op("Cphi_eopre", MASS, H.EVEN, warmup=args.warmup, reps=3, inp=src)
+        reps = int(max(20, min(args.steps, args.cpu_seconds / (probe * 1e-6))))
+        med, mn, thr = h.time_op("Cphi_eopre", MASS, H.EVEN, warmup=1, reps=reps, inp=src)
+    t = med * 1e-6
+    base = {"value": eopre_bytes(V) / t / 1e9, "unit": "GB/s", "cores": thr, "kind": "reference",
+            "sample": f"HiRep's own Cphi_eopre (libhr built from the reference sources, gcc -O3 -fopenmp, "
+                      f"OMP_PROC_BIND=close) on 16^3x32: median of {reps} applications after warm-up, "
+                      f"{med / 1e3:.2f} ms (min {mn / 1e3:.2f} ms)",
+            "note": "HiRep's Cphi_ (Dphi.c:1092-1146) shares its site temporaries between OpenMP threads, so "
+                    "with more than one thread its clover result is not reliable; the time is HiRep's"}
+    return base, t
 
 
 def reference_main(args):
@@ -164,6 +218,8 @@ def reference_main(args):
     if rank != 0:
         return
     base, t = cpu_reference_arm(args)
+    if base["kind"] == "reference":
+        base["port"] = cpu_port_arm(min(5.0, args.cpu_seconds))
     line = {"impl": "reference", "metric": METRIC, "value": base["value"],
             "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -184,6 +240,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 22-system solve (24^3x48 sextet)")
     ap.add_argument("--no-force", action="store_true", help="skip the force check (16^4 SU(4) antisymmetric)")
     ap.add_argument("--no-hmc", action="store_true", help="skip the HMC trajectory (32^3x64 SU(2) adjoint)")
+    ap.add_argument("--no-configs", action="store_true", help="skip the single-field operator at the other workloads")
     ap.add_argument("--batch-op", default=None, metavar="TxXxYxZ",
                     help="only time the batched g5Cphi_eopre of the batched workload on this lattice")
     ap.add_argument("--nb", type=int, default=12, help="fields per batch for --batch-op")
@@ -246,7 +303,18 @@ def main():
     torch.cuda.synchronize()
     with Clocks(local) as clk:
         time.sleep(0.3)  # let the sampler start
+        # one more second of untimed steps right before the timed ones: the clock
+        # record then covers the load the timed steps run under even when they
+        # last only milliseconds (the record's window is this second + the timed region)
         clk.t0 = time.time()
+        while time.time() - clk.t0 < 1.0:
+            for _ in range(50):
+                flush_l2()
+                lat.Cphi_eopre(MASS, fout, fin)
+            torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
         for a, b in evs:
             flush_l2()
             a.record(stream)
@@ -291,24 +359,32 @@ def main():
     lat.set_host_chunks(args.host_chunks)
     e2e_ms = time_e2e(e2e_pipelined)
     e2e_seq_ms = time_e2e(e2e_sequential)
+    form, ms_pipe, ms_seq = G.ctypes.c_int(), G.ctypes.c_float(), G.ctypes.c_float()
+    G._check(lat.L.hrgpu_host_form(G.ctypes.byref(form), G.ctypes.byref(ms_pipe), G.ctypes.byref(ms_seq)),
+             "host_form")
 
     solve = None
     if not args.no_solve:
         solve = run_solves(lat, fin, torch, stream, G, dist)
 
     peak, peak_kind = measured_peak()
+    ubytes = unique_bytes(lat.V, lat.nf, False, 2 if lat.link_recon() else 3, True)
     line = {
         "metric": METRIC,
         "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic", "config": workload_config(),
-        "roofline": {"bound": "hbm", "achieved": nbytes / (t_max * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
-                     "frac": nbytes / (t_max * 1e-3) / 1e9 / peak, "peak_kind": peak_kind,
-                     "kernel": "k_hop (2 launches per Cphi_eopre)", "algorithmic_bytes_per_step": nbytes,
-                     "traffic": profile_traffic()},
+        "roofline": {"bound": "hbm", "achieved": ubytes / (t_max * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": ubytes / (t_max * 1e-3) / 1e9 / peak, "peak_kind": peak_kind,
+                     "kernel": "k_hop (2 launches per Cphi_eopre)", "algorithmic_bytes_per_step": ubytes,
+                     "algorithmic_bytes": "links once per hop (two rows when rebuilt), even input x2, odd "
+                                          "temporary x2, even output, packed clover blocks once",
+                     "hirep_model_bytes_per_step": nbytes, "traffic": profile_traffic()},
         "e2e": {"value": replica_rate(nbytes, e2e_ms, world) / 1e9, "unit": "GB/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "call": f"hrgpu_apply_op_host(Cphi_eopre), pinned HiRep-layout fields, {args.host_chunks} chunks",
+                "call": "hrgpu_apply_op_host(Cphi_eopre), pinned HiRep-layout fields",
+                "form": {1: f"pipelined, {args.host_chunks} chunks", 2: "plain sequence"}.get(form.value, "eager"),
+                "form_timing_ms": {"pipelined": ms_pipe.value, "sequential": ms_seq.value},
                 "sequential_ms": e2e_seq_ms,
                 "sequential_value": replica_rate(nbytes, e2e_seq_ms, world) / 1e9},
         "gpu_launches": launches,
@@ -317,6 +393,8 @@ def main():
     }
     if solve:
         line["solve"] = solve
+    if world == 1 and not args.no_configs:
+        line["dslash_configs"] = run_dslash_configs(torch, stream, G, F, flush_l2, peak)
     if world == 1 and not args.no_batch:
         line["solve_batch"] = run_batch_solves(torch, stream, G, F)
     if world == 1 and not args.no_force:
@@ -331,6 +409,59 @@ def main():
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+# the single-field even-odd operator at the other workloads' sizes:
+# (name, dims T,X,Y,Z, NG, representation, nf, real links, clover csw, m0, eps, seed)
+DSLASH_CONFIGS = [
+    ("SU(4) antisymmetric (NF=6), Wilson Dphi_eopre, 16^4, U=exp(i0.25H) seed 11", (16, 16, 16, 16), 4, "ASYM",
+     None, -0.1, 0.25, 11),
+    ("SU(3) symmetric (NF=6), clover csw=1.0 Cphi_eopre, 24^3x48, U=exp(i0.3H) seed 21", (48, 24, 24, 24), 3, "SYM",
+     1.0, -0.3, 0.3, 21),
+    ("SU(2) adjoint (NF=3, real), Wilson Dphi_eopre, 32^3x64, U=exp(i0.2H) seed 99", (64, 32, 32, 32), 2, "ADJ",
+     None, -1.0, 0.2, 99),
+]
+
+
+def run_dslash_configs(torch, stream, G, F, flush_l2, peak, steps=50):
+    """FP64 even-odd operator per workload: device time per application (L2
+    flushed between steps, CUDA events), HiRep-model GB/s and the fraction of
+    the measured HBM peak on the bytes it must move at least."""
+    out = []
+    for name, dims, ng, rep, csw, m, eps, seed in DSLASH_CONFIGS:
+        lat = G.Lattice(*dims, ng, getattr(G, rep))
+        lat.set_gauge(F.smooth_gauge(seed, lat.V, ng, eps))
+        lat.represent_gauge_field(True)
+        if csw is not None:
+            lat.clover_init(csw)
+        real = rep == "ADJ"
+        nf = lat.nf
+        fin, fout = lat.field(G.EVEN, host=F.gaussian_spinor(seed, lat.VH, nf)), lat.field(G.EVEN)
+        op = lat.Cphi_eopre if csw is not None else lat.Dphi_eopre
+        for _ in range(5):
+            op(m, fout, fin)
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(steps):
+            flush_l2()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            op(m, fout, fin)
+            b.record(stream)
+            ts.append((a, b))
+        torch.cuda.synchronize()
+        ms = float(np.mean([a.elapsed_time(b) for a, b in ts]))
+        # HiRep's model (speed_test_diracoperator.c:82) + the clover blocks and the rho^2 input read
+        vec, link = nf * 16, nf * nf * (8 if real else 16)
+        model = lat.V * (36 * vec + 8 * link) + (lat.VH) * 4 * vec
+        if csw is not None:
+            model += lat.VH * (2 * nf * (2 * nf + 1) * 16 + 4 * nf * nf * 16)
+        rows = 2 if lat.link_recon() else nf
+        ub = unique_bytes(lat.V, nf, real, rows, csw is not None)
+        out.append({"workload": name, "ms_per_application": ms, "hirep_model_GBps": model / (ms * 1e-3) / 1e9,
+                    "algorithmic_bytes": ub, "achieved_GBps": ub / (ms * 1e-3) / 1e9,
+                    "frac_of_measured_hbm": ub / (ms * 1e-3) / 1e9 / peak, "link_rows_read": rows})
+    return out
 
 
 def hop_tuning(lat, G):

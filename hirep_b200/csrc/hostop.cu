@@ -35,6 +35,14 @@
 // S = X Y Z / 2, and a stage on a run of slabs is one launch.  Every site is
 // computed by the same kernel code as in the whole-lattice operator, so the
 // result is bit-identical to upload + operator + download.
+//
+// Whether the overlap pays depends on the host more than on the code: the
+// GPUs of a host share its PCIe and memory paths, and on some hosts the many
+// smaller copies of the pipeline lose to one copy each way.  So when a graph
+// is made for a new key, the plain sequence (one copy in, the operator on the
+// whole lattice, one copy out) is captured beside it, both are replayed and
+// timed on the spot, and the faster is kept for that key
+// (hrgpu_set_host_form pins one form, hrgpu_host_form reports the choice).
 #include <vector>
 
 #include "dirac.cuh"
@@ -55,9 +63,13 @@ struct HostPipe {
 };
 static HostPipe HP;
 static int hp_chunks = 10;  // hrgpu_set_host_chunks
+enum { FORM_AUTO = 0, FORM_PIPELINED = 1, FORM_SEQUENTIAL = 2 };
+static int hp_form = FORM_AUTO;                    // hrgpu_set_host_form
+static int hp_last_form = -1;                      // form of the last graph made
+static float hp_last_ms[2] = {-1.f, -1.f};         // its timing: pipelined, sequential
 
 struct HostGraph {
-  int clover, g5, prec, K;
+  int clover, g5, prec, K, form;
   double mass;
   const void *hin;
   void *hout;
@@ -250,6 +262,66 @@ static int enqueue_host(int clover, int g5, double mass, void *host_out, const v
   return 0;
 }
 
+// the plain sequence: one copy in, both hops on the whole lattice, one copy out
+template <typename R>
+static int enqueue_seq(int clover, int g5, double mass, void *host_out, const void *host_in, int prec) {
+  const size_t len = (size_t)L.VH * 4 * L.nf * sizeof(typename C2<R>::T);
+  const int cb1 = HP.T * HP.S;
+  HR_CUDA(cudaMemcpyAsync(HP.stage_in, host_in, len, cudaMemcpyHostToDevice, L.stream));
+  if (int rc = spinor_scatter_even(HP.din, HP.stage_in, 0, (int)L.VH, prec, L.stream)) return rc;
+  if (int rc = eo_stage<R>(clover, mass, 0, HRGPU_EVEN, HP.dout, HP.din, g5, nullptr, 0, cb1)) return rc;
+  if (int rc = eo_stage<R>(clover, mass, 1, HRGPU_EVEN, HP.dout, HP.din, g5, nullptr, 0, cb1)) return rc;
+  if (int rc = spinor_gather_even(HP.stage_out, HP.dout, 0, (int)L.VH, prec, L.stream)) return rc;
+  HR_CUDA(cudaMemcpyAsync(host_out, HP.stage_out, len, cudaMemcpyDeviceToHost, L.stream));
+  return 0;
+}
+
+// capture one form of the operator as a graph (on a private stream: the
+// library stream may be the legacy default stream, which cannot be captured)
+template <typename R>
+static int capture_form(int form, int clover, int g5, double mass, void *host_out, const void *host_in, int prec,
+                        cudaGraphExec_t *exec) {
+  cudaGraph_t graph = nullptr;
+  cudaStream_t saved = L.stream;
+  HR_CUDA(cudaStreamBeginCapture(HP.s_cap, cudaStreamCaptureModeRelaxed));
+  L.stream = HP.s_cap;
+  int rc = form == FORM_SEQUENTIAL ? enqueue_seq<R>(clover, g5, mass, host_out, host_in, prec)
+                                   : enqueue_host<R>(clover, g5, mass, host_out, host_in, prec);
+  L.stream = saved;
+  cudaError_t ce = cudaStreamEndCapture(HP.s_cap, &graph);
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (ce != cudaSuccess) return fail_cuda(ce, "apply_op_host capture", __FILE__, __LINE__);
+  ce = cudaGraphInstantiate(exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ce != cudaSuccess) return fail_cuda(ce, "apply_op_host instantiate", __FILE__, __LINE__);
+  return 0;
+}
+
+// mean time of a few replays (after one untimed), CUDA events on L.stream
+static int time_graph(cudaGraphExec_t exec, float *ms) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  int rc = 0;
+  constexpr int reps = 4;
+  if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+    rc = fail_cuda(cudaGetLastError(), "apply_op_host timing events", __FILE__, __LINE__);
+  } else {
+    cudaError_t ce = cudaGraphLaunch(exec, L.stream);
+    if (ce == cudaSuccess) ce = cudaEventRecord(a, L.stream);
+    for (int i = 0; i < reps && ce == cudaSuccess; i++) ce = cudaGraphLaunch(exec, L.stream);
+    if (ce == cudaSuccess) ce = cudaEventRecord(b, L.stream);
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(b);
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(ms, a, b);
+    if (ce != cudaSuccess) rc = fail_cuda(ce, "apply_op_host timing", __FILE__, __LINE__);
+    *ms /= reps;
+  }
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  return rc;
+}
+
 static bool pinned(const void *p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -297,23 +369,29 @@ static int apply_host(int clover, int g5, double mass, void *host_out, const voi
       if (HG.size() >= HG_MAX) free_graphs();
       if (sizeof(R) == 4 && L.flt_links == HRGPU_LINKS_BF16)
         if (int rc = ensure_links_bf16()) return rc;  // not inside the capture
-      // captured on a private stream (the library stream may be the legacy
-      // default stream, which cannot be captured) and replayed into L.stream
-      cudaGraph_t graph = nullptr;
-      cudaStream_t saved = L.stream;
-      HR_CUDA(cudaStreamBeginCapture(HP.s_cap, cudaStreamCaptureModeRelaxed));
-      L.stream = HP.s_cap;
-      int rc = enqueue_host<R>(clover, g5, mass, host_out, host_in, prec);
-      L.stream = saved;
-      cudaError_t ce = cudaStreamEndCapture(HP.s_cap, &graph);
+      cudaGraphExec_t ex[2] = {nullptr, nullptr};  // pipelined, sequential
+      int rc = 0;
+      float ms[2] = {-1.f, -1.f};
+      if (hp_form != FORM_SEQUENTIAL)
+        rc = capture_form<R>(FORM_PIPELINED, clover, g5, mass, host_out, host_in, prec, &ex[0]);
+      if (!rc && hp_form != FORM_PIPELINED)
+        rc = capture_form<R>(FORM_SEQUENTIAL, clover, g5, mass, host_out, host_in, prec, &ex[1]);
+      if (!rc && ex[0] && ex[1]) {
+        rc = time_graph(ex[0], &ms[0]);
+        if (!rc) rc = time_graph(ex[1], &ms[1]);
+      }
       if (rc) {
-        if (graph) cudaGraphDestroy(graph);
+        for (cudaGraphExec_t e : ex)
+          if (e) cudaGraphExecDestroy(e);
         return rc;
       }
-      if (ce != cudaSuccess) return fail_cuda(ce, "apply_op_host capture", __FILE__, __LINE__);
-      ce = cudaGraphInstantiate(&key.exec, graph, 0);
-      cudaGraphDestroy(graph);
-      if (ce != cudaSuccess) return fail_cuda(ce, "apply_op_host instantiate", __FILE__, __LINE__);
+      const int keep = !ex[0] ? 1 : !ex[1] ? 0 : (ms[1] < ms[0] ? 1 : 0);
+      if (ex[1 - keep]) cudaGraphExecDestroy(ex[1 - keep]);
+      key.exec = ex[keep];
+      key.form = keep ? FORM_SEQUENTIAL : FORM_PIPELINED;
+      hp_last_form = key.form;
+      hp_last_ms[0] = ms[0];
+      hp_last_ms[1] = ms[1];
       HG.push_back(key);
       hit = &HG.back();
     }
@@ -333,6 +411,20 @@ extern "C" {
 int hrgpu_set_host_chunks(int chunks) {
   HR_REQUIRE(chunks >= 1, HRGPU_E_ARG, "set_host_chunks: chunks must be >= 1");
   hp_chunks = chunks;
+  return 0;
+}
+
+int hrgpu_set_host_form(int form) {
+  HR_REQUIRE(form >= FORM_AUTO && form <= FORM_SEQUENTIAL, HRGPU_E_ARG, "set_host_form: form %d is not 0, 1 or 2", form);
+  if (form != hp_form) free_graphs();
+  hp_form = form;
+  return 0;
+}
+
+int hrgpu_host_form(int *form, float *ms_pipelined, float *ms_sequential) {
+  if (form) *form = hp_last_form;
+  if (ms_pipelined) *ms_pipelined = hp_last_ms[0];
+  if (ms_sequential) *ms_sequential = hp_last_ms[1];
   return 0;
 }
 

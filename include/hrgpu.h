@@ -194,6 +194,15 @@ int hrgpu_D(void *out, const void *in);
  * overlap. */
 int hrgpu_apply_op_host(int op, double mass, void *host_out, const void *host_in, int prec);
 int hrgpu_set_host_chunks(int chunks); /* chunks of the pipeline (default 10; 1 = no overlap) */
+/* With pinned buffers the operator runs as a cached CUDA graph per (operator,
+ * mass, buffers, ...).  Form 0 (default): when a graph is made, the pipelined
+ * form and the plain sequence (one copy each way around the whole-lattice
+ * operator) are both captured and timed, and the faster is kept; 1 forces the
+ * pipeline, 2 the plain sequence.  No HiRep counterpart (host-field transport). */
+int hrgpu_set_host_form(int form);
+/* the form chosen for the last graph made (1 pipelined, 2 sequential, -1 none
+ * yet) and the replay times measured for that choice (ms; -1 if not timed) */
+int hrgpu_host_form(int *form, float *ms_pipelined, float *ms_sequential);
 
 /* ---------------------------------------------------------------- clover -- */
 int hrgpu_clover_init(double csw);                  /* clover_init, clover_tools.c:360-373        */

@@ -17,7 +17,9 @@ count, in clover builds the clover term of the first two sites and the squared
 norm of all of it, and the force (force_fermion_core + fermion_force_end,
 dt 0.37, residue 1.3).  The geometry fixture holds ipt/iup/idn of a 4x6x2x8
 lattice; config1.npz holds the average plaquette of HiRep's hot start
-(random_u after rlxd_init(1, 1234), 8^4).
+(random_u after rlxd_init(1, 1234), 8^4) drawn by one OpenMP thread: ranlxd
+keeps one stream per thread (LibHR/Random/ranlxd.c:459-470) and random_u draws
+inside a parallel site loop, so the field depends on the thread count.
 """
 import os
 import sys
@@ -70,7 +72,7 @@ def main():
     with H.HiRep("su3_fund", 4, 6, 2, 8) as h:
         ipt, iup, idn = h.geometry()
     np.savez_compressed(os.path.join(HERE, "hirep_geometry_4x6x2x8.npz"), ipt=ipt, iup=iup, idn=idn)
-    with H.HiRep("su3_fund", 8, 8, 8, 8, seed=1234) as h:
+    with H.HiRep("su3_fund", 8, 8, 8, 8, seed=1234, threads=1) as h:
         h.random_u()
         plaq = h.plaquette()
     np.savez_compressed(os.path.join(HERE, "hirep_config1.npz"), plaquette=np.float64(plaq))

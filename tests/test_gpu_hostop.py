@@ -129,3 +129,37 @@ def test_apply_op_host_graph_path_with_pinned_buffers():
     lat.represent_gauge_field(True)  # rebuilds the clover term
     check(-0.2, 3)
     check(-0.1, 4)  # a new mass: a new graph
+
+
+@pytest.mark.parametrize("form", [0, 1, 2])
+def test_apply_op_host_forms_are_bit_identical(form):
+    """Form 0 times the pipelined form against the plain sequence when it makes a
+    graph and keeps the faster; 1 and 2 pin one.  Every form gives the device
+    operator's field bit for bit, and the choice is reported."""
+    import torch
+
+    o, u, lat = make((8, 4, 4, 4), 3, O.FUND)
+    G._check(lat.L.hrgpu_set_host_form(form), "set_host_form")
+    try:
+        n = lat.VH * 4 * lat.nf
+        t_in = torch.empty(2 * n, dtype=torch.float64).pin_memory()
+        t_out = torch.empty(2 * n, dtype=torch.float64).pin_memory()
+        h_in = t_in.numpy().view(np.complex128).reshape(lat.VH, 4, lat.nf)
+        h_out = t_out.numpy().view(np.complex128).reshape(lat.VH, 4, lat.nf)
+        h_in[...] = F.gaussian_spinor(21, lat.VH, lat.nf)
+        fin, fout = lat.field(G.EVEN, host=h_in.copy()), lat.field(G.EVEN)
+        lat.Cphi_eopre(-0.2, fout, fin)  # settles the kernel variants: the graph path
+        for _ in range(2):
+            lat.apply_op_host(G.OP_CPHI_EOPRE, -0.2, h_in, out=h_out)
+            assert np.array_equal(h_out, fout.download())
+        chosen, ms_p, ms_s = G.ctypes.c_int(), G.ctypes.c_float(), G.ctypes.c_float()
+        G._check(lat.L.hrgpu_host_form(G.ctypes.byref(chosen), G.ctypes.byref(ms_p), G.ctypes.byref(ms_s)), "form")
+        if form == 0:
+            assert chosen.value in (1, 2) and ms_p.value > 0 and ms_s.value > 0
+            assert chosen.value == (2 if ms_s.value < ms_p.value else 1)
+        else:
+            assert chosen.value == form
+    finally:
+        G._check(lat.L.hrgpu_set_host_form(0), "set_host_form")
+    with pytest.raises(G.HRGPUError, match="set_host_form"):
+        G._check(lat.L.hrgpu_set_host_form(3), "set_host_form")

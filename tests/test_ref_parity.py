@@ -216,7 +216,7 @@ def test_config1_hot_start_from_hireps_ranlux():
     """Config 1 as specified: SU(3) fundamental 8^4, random_u after rlxd_init(1,1234),
     Dphi / Dphi_eopre at m0=0.1, and CG on g5Dphi_sq to |r|/|b| < 1e-14."""
     dims, m = (8, 8, 8, 8), 0.1
-    with H.HiRep("su3_fund", *dims, seed=1234) as h:
+    with H.HiRep("su3_fund", *dims, seed=1234, threads=1) as h:
         u = h.random_u()
         plaq = h.plaquette()
         f = h.gaussian_spinor_field(H.FULL)
@@ -229,8 +229,11 @@ def test_config1_hot_start_from_hireps_ranlux():
     # back already carry the antiperiodic sign (archive.c:238-242)
     o.set_gauge(o.represent_gauge_field(u, False))
     o.set_mass(m)
-    # a hot start: the average plaquette of Haar links is ~0
+    # a hot start: the average plaquette of Haar links is ~0; one thread draws
+    # the fixture's field (ranlxd keeps a stream per OpenMP thread)
     assert abs(plaq) < 0.02
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "hirep_config1.npz"))
+    assert abs(plaq - float(g["plaquette"])) < 1e-14
     assert abs(o.avr_plaquette(u) - plaq) < 1e-12
     assert rel(o.Dphi(m, f), d_h) < 1e-13
     assert rel(o.Dphi_eopre(m, e), eo_h) < 1e-13
