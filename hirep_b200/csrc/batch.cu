@@ -819,7 +819,7 @@ static int bcg_core(int op, double mass, int nb, int ns, const int *src, const d
   if (bad >= 0) {
     set_error("cg_mshift_batch: breakdown of source %d at iteration %d (alpha=%g, |r|^2=%g)", bad, h.s[bad].iter,
               h.s[bad].alpha, h.s[bad].lambda);
-    return HRGPU_E_NOCONV;
+    return HRGPU_E_BREAKDOWN;
   }
   return 0;
 }
@@ -953,6 +953,9 @@ int hrgpu_cg_mshift_batch(int op, double mass, int nsrc, const int *nshift, cons
   HR_CUDA(cudaMemcpyAsync(BO.d_shift, shift, sizeof(double) * ns, cudaMemcpyHostToDevice, L.stream));
   std::vector<double> innorm2(nsrc), norm(ns);
   if (int rc = bdot_host(BO.b, BO.b, HRGPU_DOUBLE, rows, nsrc, BO.part, BO.dres, BO.hres_h, innorm2.data())) return rc;
+  for (int s = 0; s < nsrc; s++)
+    HR_REQUIRE(isfinite(innorm2[s]), HRGPU_E_BREAKDOWN, "cg_mshift_batch: the norm of source %d is not finite (%g)", s,
+               innorm2[s]);
   int status = 0;
 
   if (!flt) {
@@ -962,6 +965,9 @@ int hrgpu_cg_mshift_batch(int op, double mass, int nsrc, const int *nshift, cons
                                   BO.x, iters))
       return rc;
     if (int rc = bresidual(op, mass, nsrc, ns, rows, norm.data())) return rc;
+    for (int j = 0; j < ns; j++)
+      HR_REQUIRE(isfinite(norm[j]), HRGPU_E_BREAKDOWN, "cg_mshift_batch: the residual of system %d is not finite (%g)",
+                 j, norm[j]);
     for (int j = 0; j < ns; j++) {
       iters[src[j]]++;
       flags[j] = (innorm2[src[j]] == 0.0 || norm[j] / innorm2[src[j]] <= err2) ? 1 : 0;
@@ -994,6 +1000,9 @@ int hrgpu_cg_mshift_batch(int op, double mass, int nsrc, const int *nshift, cons
   int rounds = 0;
   for (;;) {
     if (int rc = bresidual(op, mass, nsrc, ns, rows, norm.data())) return rc;
+    for (int j = 0; j < ns; j++)
+      HR_REQUIRE(isfinite(norm[j]), HRGPU_E_BREAKDOWN, "cg_mshift_batch: the residual of system %d is not finite (%g)",
+                 j, norm[j]);
     std::vector<int> todo;
     for (int j = 0; j < ns; j++) {
       const int s = src[j];

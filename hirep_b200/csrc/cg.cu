@@ -367,6 +367,16 @@ static int cg_core(int op, double mass, int n, const double *shift, double err2,
   int cgiter = 0;
   double innorm2;
   if (int rc = la_dot(2, par, prec, in, nullptr, &innorm2)) return rc;
+  if (!isfinite(innorm2)) {
+    *iters = 0;
+    set_error("cg_mshift: the source norm is not finite (%g)", innorm2);
+    return HRGPU_E_BREAKDOWN;
+  }
+  if (innorm2 == 0.0) {  // (M - s_i) x = 0: every solution is zero, nothing to iterate
+    for (int i = 0; i < n; i++) HR_CUDA(cudaMemsetAsync(out[i], 0, bytes, L.stream));
+    *iters = 0;
+    return 0;
+  }
   if (n == 1) {
     // out[0] is the initial guess
     if (int rc = apply_op(op, prec, mass, Mk, out[0])) return rc;
@@ -428,7 +438,7 @@ static int cg_core(int op, double mass, int n, const double *shift, double err2,
   if (h.state == 3) {
     *iters = cgiter;
     set_error("cg_mshift: breakdown at iteration %d (alpha=%g, |r|^2=%g)", cgiter, h.alpha, h.lambda);
-    return HRGPU_E_NOCONV;
+    return HRGPU_E_BREAKDOWN;
   }
   if (!flt) {
     // true residual of every shift (cg_mshift.c:122-137)
@@ -439,6 +449,11 @@ static int cg_core(int op, double mass, int n, const double *shift, double err2,
       if (int q = la_op(LA_SUB_ASSIGN, par, prec, Mk, in, nullptr, 0, 0, 0, 0)) return q;
       double nr;
       if (int q = la_dot(2, par, prec, Mk, nullptr, &nr)) return q;
+      if (!isfinite(nr)) {
+        *iters = cgiter;
+        set_error("cg_mshift: the true residual of shift %d is not finite (%g)", i, nr);
+        return HRGPU_E_BREAKDOWN;
+      }
       flags[i] = (fabs(nr / innorm2) > err2) ? 0 : 1;
     }
   }
@@ -522,6 +537,16 @@ int hrgpu_cg_mshift_flt(int op, double mass, int n, const double *shift, double 
     if (n != 1) HR_CUDA(cudaMemsetAsync(out[i], 0, bd, L.stream));
   double innorm2;
   if (int rc = la_dot(2, par, HRGPU_DOUBLE, in, nullptr, &innorm2)) return rc;
+  if (!isfinite(innorm2)) {
+    *iters = 0;
+    set_error("cg_mshift_flt: the source norm is not finite (%g)", innorm2);
+    return HRGPU_E_BREAKDOWN;
+  }
+  if (innorm2 == 0.0) {
+    for (int i = 0; i < n; i++) HR_CUDA(cudaMemsetAsync(out[i], 0, bd, L.stream));
+    *iters = 0;
+    return 0;
+  }
   int siter = 0, diter = 0, notconverged, rounds = 0;
   const double mass_d = mass;
   do {
@@ -535,6 +560,11 @@ int hrgpu_cg_mshift_flt(int op, double mass, int n, const double *shift, double 
       if (int rc = la_op(LA_SUB, par, HRGPU_DOUBLE, dres2, in, dtmp, 0, 0, 0, 0)) return rc;
       if (int rc = la_op(LA_MUL_ADD_ASSIGN, par, HRGPU_DOUBLE, dres2, out[i], nullptr, shift[i], 0, 0, 0)) return rc;
       if (int rc = la_dot(2, par, HRGPU_DOUBLE, dres2, nullptr, &norm[i])) return rc;
+      if (!isfinite(norm[i])) {
+        *iters = siter + diter;
+        set_error("cg_mshift_flt: the residual of shift %d is not finite (%g)", i, norm[i]);
+        return HRGPU_E_BREAKDOWN;
+      }
       if (norm[i] < innorm2 * err2) {
         sflags[i] = 0;
         norm[i] /= innorm2;

@@ -45,6 +45,7 @@ int hop(int outp, void *out, const void *in, int ep, double cacc, const void *au
   a.outp = outp;
   a.g5 = g5;
   a.stop = L.cur_stop;
+  a.err = nullptr;
   if (sizeof(R) == 4 && L.flt_links == HRGPU_LINKS_BF16) {
     if (int rc = ensure_links_bf16()) return rc;
     a.U = L.Ubf;

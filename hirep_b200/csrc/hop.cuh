@@ -35,6 +35,7 @@ struct HopArgs {
   const typename C2<R>::T *cod;  // packed clover off-diagonal [2][NF(2NF-1)][2ld]
   double *red;       // block partials of |out|^2 (or nullptr)
   const int *stop;   // inverter state: when non-null and *stop != 0 the launch does nothing
+  unsigned *err;     // device error word (variant 5: bit 0 = a bounded wait gave up), or nullptr
   R cacc, caux;
   int outp;
   int g5;

@@ -156,6 +156,38 @@ int launch_ep_variant(HopArgs<R> &a, int variant) {
   return 0;
 }
 
+// variant 5 (pinned with hrgpu_set_hop_variant): the launch gets the device
+// error word, and outside a stream capture the word is read back at once, so a
+// bounded wait that gave up (copies possibly still in flight into shared
+// memory) is reported as an error status instead of passing silently
+template <typename R, int EP>
+int launch_tma_checked(HopArgs<R> &a) {
+  if (!L.hop_err) {
+    HR_CUDA(cudaMalloc(&L.hop_err, sizeof(unsigned)));
+    HR_CUDA(cudaMemsetAsync(L.hop_err, 0, sizeof(unsigned), L.stream));
+  }
+  a.err = L.hop_err;
+  int rc = launch_ep_variant<R, EP>(a, 5);
+  a.err = nullptr;
+  if (rc < 0) {
+    set_error("hopping-kernel variant 5 is not built for NF=%d (or this lattice)", L.nf);
+    return HRGPU_E_NF;
+  }
+  if (rc) return rc;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  HR_CUDA(cudaStreamIsCapturing(L.stream, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return 0;
+  unsigned h = 0;
+  HR_CUDA(cudaMemcpyAsync(&h, L.hop_err, sizeof(unsigned), cudaMemcpyDeviceToHost, L.stream));
+  HR_CUDA(cudaStreamSynchronize(L.stream));
+  if (h) {
+    HR_CUDA(cudaMemsetAsync(L.hop_err, 0, sizeof(unsigned), L.stream));
+    set_error("hopping-kernel variant 5: a bounded wait for the staged time halo gave up (error word %u)", h);
+    return HRGPU_E_CUDA;
+  }
+  return 0;
+}
+
 // Autotuner: the first launch of each (precision, epilogue) on a lattice times
 // every variant on the real arguments (3 launches each, CUDA events on the
 // library stream) and keeps the faster one.  The output is rewritten by the
@@ -167,6 +199,7 @@ int launch_ep(HopArgs<R> &a) {
   const int pi = sizeof(R) == 8 ? 0 : (L.flt_links == HRGPU_LINKS_BF16 ? 2 : 1);
   int &v = L.hop_variant[pi][EP];
   if (L.hop_force >= 0) {
+    if (L.hop_force == 5) return launch_tma_checked<R, EP>(a);
     int rc = launch_ep_variant<R, EP>(a, L.hop_force);
     if (rc < 0) {
       set_error("hopping-kernel variant %d is not built for NF=%d", L.hop_force, L.nf);
@@ -198,6 +231,10 @@ int launch_ep(HopArgs<R> &a) {
     // the events are destroyed on every way out of the loop
     auto tune = [&]() -> int {
       for (int cand = 0; cand < HOP_VARIANTS; cand++) {
+        if (cand == 5) {  // the TMA-staged variant: slower in every measured case, pinned only
+          L.hop_tune_ms[pi][EP][cand] = -1.0f;
+          continue;
+        }
         int rc0 = launch_ep_variant<R, EP>(a, cand);  // warm-up
         if (rc0 < 0) {  // variant not built for this NF
           L.hop_tune_ms[pi][EP][cand] = -1.0f;

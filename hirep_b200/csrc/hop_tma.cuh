@@ -10,8 +10,12 @@
 // memory; the t direction comes last, from shared memory.  Each wait on the
 // mbarrier is bounded: a thread that gives up reads its t neighbours from
 // global memory instead (the same values), and the block waits again, bounded,
-// before it exits so that no copy lands in released shared memory.  No
-// multicast: every copy reads this GPU's own memory into this block.
+// before it exits so that no copy lands in released shared memory; if that
+// last wait gives up, the block sets bit 0 of the launch's error word, which
+// the launcher turns into an error status.  No multicast: every copy reads
+// this GPU's own memory into this block.  Measured slower than variant 0 in
+// every case, the variant is not among the autotuner's candidates; it runs
+// only when pinned with hrgpu_set_hop_variant(5).
 #pragma once
 #include "hop_async.cuh"
 
@@ -69,7 +73,11 @@ __global__ void __launch_bounds__(HOP_THREADS) k_hop_tma(HopArgs<R> a) {
   const double nrm = hop_site<NFT, REAL, R, EP, typename LinkE<REAL, R>::T, true>(
       a, cb0 + threadIdx.x, sup + threadIdx.x, sdn + threadIdx.x, bar_a);
   if (a.red) block_partial<R>(nrm, a.red);
-  tma_wait(bar_a);  // at once when the copies were seen; bounded otherwise
+  // at once when the copies were seen; bounded otherwise.  A block that gives
+  // up here may leave copies in flight into shared memory the next resident
+  // block reuses, so the launch is reported as failed (the launcher reads the
+  // word back after every launch of this variant)
+  if (!tma_wait(bar_a) && a.err) atomicOr(a.err, 1u);
 }
 
 }  // namespace hrgpu

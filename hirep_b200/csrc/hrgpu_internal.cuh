@@ -108,6 +108,7 @@ struct Lattice {
   // tuned hopping-kernel variant [FP64, FP32, FP32 with BF16 links][epilogue]
   int hop_variant[3][3] = {{-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}};
   int hop_force = -1;             // forced variant (-1: autotune)
+  unsigned *hop_err = nullptr;    // device error word of the TMA-staged variant
   bool hop_pdl = true;            // whole-lattice hops with programmatic dependent launch
   float hop_tune_ms[3][3][HOP_VARIANTS] = {};  // tuning times of the variants [slot][epilogue][variant]
   // storage of the links read by the FP32 operators: HRGPU_LINKS_F32 (Uf) or HRGPU_LINKS_BF16 (Ubf)
@@ -137,6 +138,7 @@ inline size_t spinor_bytes(int par, int prec) {
 }
 
 int ensure_tmp(void **p, size_t bytes);
+int library_device();  // the device of hrgpu_init (-1 before)
 int ensure_links_bf16();  // the BF16 copy of the links, made from the FP64 ones when they changed
 int detect_recon12();     // check links set already represented for row-2 reconstruction
 int compute_clover_term_dev();

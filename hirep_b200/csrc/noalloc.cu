@@ -39,9 +39,16 @@ static __device__ __align__(256) double2 g_noalloc_scratch[NOALLOC_SCRATCH_BYTES
 constexpr int MAX_DEVICES = 64;
 static void *g_scratch_addr[MAX_DEVICES] = {nullptr};
 
+// The lookup is made with the library's own device current (the one its
+// stream and lattice live on): a caller whose framework left another device
+// current is refused, rather than handed an address on the wrong GPU (or a
+// second 32 MiB reservation on it).
 static int scratch_address(void **p) {
   int dev = -1;
   HR_CUDA(cudaGetDevice(&dev));
+  HR_REQUIRE(dev == library_device(), HRGPU_E_STATE,
+             "Dphi_eopre_noalloc: device %d is current, but the library runs on device %d (make it current first)",
+             dev, library_device());
   HR_REQUIRE(dev >= 0 && dev < MAX_DEVICES, HRGPU_E_ARG, "Dphi_eopre_noalloc: device %d out of range", dev);
   if (!g_scratch_addr[dev]) {
     void *a = nullptr;

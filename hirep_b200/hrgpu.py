@@ -20,6 +20,7 @@ FUND, ADJ, SYM, ASYM = 0, 1, 2, 3
 OP_G5DPHI_SQ, OP_G5DPHI_EOPRE_SQ, OP_G5CPHI_EOPRE_SQ, OP_G5CPHI_SQ = 0, 1, 2, 3
 OP_DPHI_EOPRE, OP_G5DPHI_EOPRE, OP_CPHI_EOPRE, OP_G5CPHI_EOPRE, OP_DPHI, OP_CPHI = 4, 5, 6, 7, 8, 9
 E_NOCONV = 5
+E_BREAKDOWN = 6
 LINKS_F32, LINKS_BF16 = 0, 1
 
 _lib = None

@@ -56,7 +56,10 @@ enum {
   HRGPU_E_ARG = 2,       /* invalid argument                            */
   HRGPU_E_STATE = 3,     /* called before the state it needs was set    */
   HRGPU_E_NF = 4,        /* no kernel instantiated for this NF          */
-  HRGPU_E_NOCONV = 5     /* inverter stopped at max_iter (not fatal)    */
+  HRGPU_E_NOCONV = 5,    /* inverter stopped at max_iter (not fatal)    */
+  HRGPU_E_BREAKDOWN = 6  /* inverter breakdown: a non-finite source, norm or
+                            residual, or zero curvature <p, M p> (a NaN field or a
+                            singular system); the solution is garbage (fatal)  */
 };
 
 /* ---------------------------------------------------------------- setup -- */

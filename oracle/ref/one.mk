@@ -65,3 +65,42 @@ $(GEN)/approx_data.db:
 	cd $(REF)/LibHR/Update/remez && cat approx_* | perl ./mkappdata.pl > $@
 
 .PHONY: all
+
+# ---------------------------------------------------------------------------
+# HiRep's own check programs linked through the drop-in binding
+# (hirep_b200/shim/hrgpu_hirep.c) to the GPU library: the replaced functions
+# are redirected with the linker's --wrap, HiRep's sources stay as they are.
+# Needs hirep_b200/libhrgpu.so built first.
+SHIM     := $(abspath ../../hirep_b200/shim/hrgpu_hirep.c)
+GPULIB   := $(abspath ../../hirep_b200)
+CUDA     ?= /usr/local/cuda
+CHECKS   := DiracOperator/check_diracoperator_1 DiracOperator/check_diracoperator_3 \
+            DiracOperator/check_diracoperator_6 Inverters/check_inverters_1 Inverters/check_inverters_6
+WRAPPED  := represent_gauge_field compute_clover_term set_dirac_mass getMVM Dphi_ Dphi g5Dphi g5Dphi_sq \
+            Dphi_eopre Dphi_oepre g5Dphi_eopre g5Dphi_eopre_sq Dphi_flt_ Dphi_flt g5Dphi_flt g5Dphi_sq_flt \
+            Dphi_eopre_flt g5Dphi_eopre_flt g5Dphi_eopre_sq_flt Cphi g5Cphi g5Cphi_sq Cphi_eopre g5Cphi_eopre \
+            g5Cphi_eopre_sq Cphi_diag Cphi_diag_inv cg_mshift fermion_force_begin force_fermion_core fermion_force_end
+SHIMEXE  := $(foreach c,$(CHECKS),$(OUT)/$(CFG)/shim/$(notdir $(c)))
+
+shim: $(SHIMEXE)
+
+$(B)/shim/hrgpu_hirep.o: $(SHIM) $(HDRS) ../../include/hrgpu.h
+	@mkdir -p $(dir $@)
+	gcc $(CFLAGS) $(CPP) $(INC) -I../../include -I$(CUDA)/include -c $< -o $@
+
+$(B)/shim/%.o: $(REF)/TestProgram/DiracOperator/%.c $(HDRS)
+	@mkdir -p $(dir $@)
+	gcc $(CFLAGS) $(CPP) $(INC) -c $< -o $@
+
+$(B)/shim/%.o: $(REF)/TestProgram/Inverters/%.c $(HDRS)
+	@mkdir -p $(dir $@)
+	gcc $(CFLAGS) $(CPP) $(INC) -c $< -o $@
+
+$(OUT)/$(CFG)/shim/%: $(B)/shim/%.o $(B)/shim/hrgpu_hirep.o $(B)/libhr.a $(GPULIB)/libhrgpu.so
+	@mkdir -p $(dir $@)
+	gcc -fopenmp -o $@ $< $(B)/shim/hrgpu_hirep.o $(B)/libhr.a $(addprefix -Wl$(comma)--wrap=,$(WRAPPED)) \
+	    -L$(GPULIB) -lhrgpu -L$(CUDA)/lib64 -lcudart -lm \
+	    -Wl,-rpath,'$$ORIGIN/../../../../hirep_b200' -Wl,-rpath,$(CUDA)/lib64
+
+comma := ,
+.PHONY: shim
