@@ -241,6 +241,8 @@ def main():
     ap.add_argument("--no-force", action="store_true", help="skip the force check (16^4 SU(4) antisymmetric)")
     ap.add_argument("--no-hmc", action="store_true", help="skip the HMC trajectory (32^3x64 SU(2) adjoint)")
     ap.add_argument("--no-configs", action="store_true", help="skip the single-field operator at the other workloads")
+    ap.add_argument("--force-only", action="store_true",
+                    help="only the force leg, without finite differences (for profiling its kernels)")
     ap.add_argument("--batch-op", default=None, metavar="TxXxYxZ",
                     help="only time the batched g5Cphi_eopre of the batched workload on this lattice")
     ap.add_argument("--nb", type=int, default=12, help="fields per batch for --batch-op")
@@ -265,6 +267,9 @@ def main():
     torch.cuda.set_device(local)
     if args.batch_op:
         return batch_op_main(args, torch, G, F)
+    if args.force_only:
+        print(json.dumps({"force": run_force_check(torch, torch.cuda.current_stream(), G, F, fd=())}), flush=True)
+        return
     dist = None
     if world > 1:
         import datetime
@@ -544,18 +549,22 @@ B_DIMS, B_NG, B_MASS, B_CSW, B_EPS, B_SEED = (48, 24, 24, 24), 3, -0.3, 1.0, 0.3
 F_DIMS, F_NG, F_MASS, F_EPS, F_SEED = (16, 16, 16, 16), 4, -0.1, 0.25, 11
 
 
-def run_force_check(torch, stream, G, F, ndir=4, step=1e-3):
-    """Pseudofermion force: kernel time, and its error against central differences of S
-    (fourth-order stencil) along ndir random su(4) directions on every link; FP64
-    solves to err2 = 1e-28.  S is about 8e5 here and a solve leaves it about 1e-8
-    uncertain, so the step is 1e-3 (truncation of the stencil ~ step^4 / 30).
-    Also the force from an X solved by the FP32-inner defect-correction CG,
-    against the FP64 force."""
+def run_force_check(torch, stream, G, F, fd=((4, 1e-3), (4, 1e-4), (32, 1e-5))):
+    """Pseudofermion force: kernel time, its roofline, and its error against
+    central differences of S (fourth-order stencil) along random su(4)
+    directions on every link, for each (number of directions, step) of fd; FP64
+    solves to err2 = 1e-28.  S is about 8e5 here and a solve leaves it about
+    1e-8 uncertain, so the error at small steps measures the solver, at large
+    ones the stencil's truncation (~ step^4 / 30): the steps are reported side
+    by side.  The links are moved on the device (U <- exp(eps i w.T) U with the
+    direction w as momenta, update_gauge_field).  Also the force from an X
+    solved by the FP32-inner defect-correction CG, against the FP64 force."""
     lat = G.Lattice(*F_DIMS, F_NG, G.ASYM)
     u0 = F.smooth_gauge(F_SEED, lat.V, F_NG, F_EPS)
     lat.set_gauge(u0)
     lat.represent_gauge_field(True)
     nf, V, VH = lat.nf, lat.V, lat.VH
+    dimg = F_NG * F_NG - 1
     g5 = np.array([1, 1, -1, -1])[None, :, None]
     eta = F.gaussian_spinor(F_SEED, VH, nf)
     fe, tmp = lat.field(G.EVEN, host=g5 * eta), lat.field(G.EVEN)
@@ -563,7 +572,6 @@ def run_force_check(torch, stream, G, F, ndir=4, step=1e-3):
     phi = lat.field(G.EVEN, host=g5 * tmp.download())
     x, y = lat.field(G.EVEN), lat.field(G.EVEN)
     op = G.OP_G5DPHI_EOPRE_SQ
-    gT = lat.generators()
 
     def solve(flt=False, err2=1e-28):
         lat.la("zero", x)
@@ -571,19 +579,22 @@ def run_force_check(torch, stream, G, F, ndir=4, step=1e-3):
         assert ok
         return lat.prod_re(phi, x)
 
+    Xs = np.zeros((V, 4, nf), complex)
+    Ys = np.zeros_like(Xs)
+    fX, fY = lat.field(G.FULL), lat.field(G.FULL)
+
     def force():
         lat.g5Dphi_eopre(F_MASS, y, x)
-        Xs = np.zeros((V, 4, nf), complex)
-        Ys = np.zeros_like(Xs)
         Xs[:VH], Ys[:VH] = y.download(), x.download()
-        fX, fY = lat.field(G.FULL, host=Xs), lat.field(G.FULL, host=Ys)
+        fX.upload(Xs)
+        fY.upload(Ys)
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         lat.fermion_force_begin()
         a.record(stream)
         lat.force_fermion_core(fX, fY, 1, 1.0, 1.0)
         b.record(stream)
-        f = lat.fermion_force_end(1.0, np.zeros((V, 4, F_NG * F_NG - 1)))
+        f = lat.fermion_force_end(1.0, np.zeros((V, 4, dimg)))
         return f, a.elapsed_time(b)
 
     torch.cuda.synchronize()
@@ -595,30 +606,44 @@ def run_force_check(torch, stream, G, F, ndir=4, step=1e-3):
     solve(flt=True, err2=1e-26)
     f32, _ = force()
     rng = np.random.default_rng(32)
-    worst = 0.0
-    flat = u0.reshape(V * 4, F_NG, F_NG)
-    for _ in range(ndir):
-        w = rng.standard_normal((V * 4, F_NG * F_NG - 1))
+    fd_out = []
+    for ndir, step in fd:
+        worst = 0.0
+        for _ in range(ndir):
+            w = rng.standard_normal((V, 4, dimg))
 
-        def action(eps):
-            X = np.einsum("ka,aij->kij", eps * w, gT)
-            u = np.einsum("kij,kjl->kil", F.exp_i_hermitian(X), flat)
-            lat.set_gauge(u.reshape(V, 4, F_NG, F_NG))
-            lat.represent_gauge_field(True)
-            return solve()
+            def action(eps):
+                lat.set_gauge(u0)
+                lat.momenta_set(w)
+                lat.update_gauge_field(eps)  # U <- exp(eps i w.T) U, represented again
+                return solve()
 
-        s1 = action(step) - action(-step)
-        s2 = action(2 * step) - action(-2 * step)
-        fd = (8 * s1 - s2) / (12 * step)
-        an = float(-0.5 * np.sum(w * f64.reshape(V * 4, -1)))
-        worst = max(worst, abs(fd - an) / abs(an))
+            s1 = action(step) - action(-step)
+            s2 = action(2 * step) - action(-2 * step)
+            fd_val = (8 * s1 - s2) / (12 * step)
+            an = float(-0.5 * np.sum(w * f64))
+            worst = max(worst, abs(fd_val - an) / abs(an))
+        fd_out.append({"directions": ndir, "step": step, "max_rel_err_fp64": worst})
     lat.set_gauge(u0)
     lat.represent_gauge_field(True)
+    # the bytes the force must move at least: X and Y (full lattice), every
+    # link once, the force planes read and written; plus the two odd-site fill
+    # hops (links once each, the even half read, the odd half written)
+    spin = 4 * nf * 16
+    core_bytes = 2 * V * spin + 4 * V * nf * nf * 16 + 2 * 4 * V * dimg * 8
+    fill_bytes = 2 * (4 * V * nf * nf * 16 + 2 * VH * spin)
+    peak, _ = measured_peak()
     return {"workload": "SU(4) antisymmetric (NF=6), Wilson m0=-0.1, 16^4, U=exp(i0.25H) seed 11, "
                         "phi = D^+ eta; S = phi^+ (H^2)^-1 phi",
             "force_fermion_core_ms": core_ms, "fp64_solve_s": solve_s,
-            "fd": f"{ndir} random su(4) directions on all links, 4th-order central differences, step {step}",
-            "fd_max_rel_err_fp64": worst,
+            "algorithmic_bytes": core_bytes + fill_bytes,
+            "algorithmic_bytes_note": "X, Y, links and force planes (read + write) of the core, plus the two "
+                                      "odd-site fill hops",
+            "achieved_GBps": (core_bytes + fill_bytes) / (core_ms * 1e-3) / 1e9,
+            "frac_of_measured_hbm": (core_bytes + fill_bytes) / (core_ms * 1e-3) / 1e9 / peak,
+            "fd": fd_out,
+            "fd_method": "random su(4) directions on all links, 4th-order central differences",
+            "fd_max_rel_err_fp64": max((r["max_rel_err_fp64"] for r in fd_out), default=None),
             "mixed_vs_fp64_force_rel_err": float(np.abs(f32 - f64).max() / np.abs(f64).max())}
 
 

@@ -79,7 +79,9 @@ __device__ __forceinline__ void f_dir(double2 (&s1)[N * N], const void *U, long 
     }
 }
 
-// force_fermion_core hopping part (force_fermion_core.c:848-923)
+// force_fermion_core hopping part (force_fermion_core.c:848-923), one thread per
+// link with the projections and s1 in registers: the form kept for the
+// representations k_force_hop_w does not cover (complex NF > 6, real NF > 3)
 template <int N, bool REAL>
 __global__ void k_force_hop(double *fsum, const void *U, const double2 *X, const double2 *Y, Geo g, ProjTab P,
                             double coeff) {
@@ -97,6 +99,119 @@ __global__ void k_force_hop(double *fsum, const void *U, const double2 *X, const
   f_dir<N, REAL>(s1, U, lp, mu, d, dy, X, Y, g.ld);
   f_dir<N, REAL>(s1, U, lp, mu, d, dy, Y, X, g.ld);
   project_add<N>(s1, P, fsum, lp, mu, d, coeff);
+}
+
+// The same hopping force with the link pulled out of the outer products.  Per
+// link (x, mu) HiRep forms s1 = sum of four terms (U A_k) B_k^+, k over the two
+// spin projections of the two pairings (X at x with Y at x+mu, and Y at x with
+// X at x+mu): A_k are projections at x+mu, B_k at x (_F_DIRmu,
+// force_fermion_core.c:72-114).  Here the four U A_k are formed first (the
+// link read once, row by row), then the B_k, and each element s1_ij is built
+// from them and at once projected onto the algebra, element by element, with
+// the table by element (its A and coefficient pairs).  So neither s1 nor the
+// projections of the old form live in registers together, every array index is
+// known at compile time (no local memory), and the per-generator sums go to a
+// column of shared memory owned by the thread; the force planes get one
+// read-modify-write per generator at the end.  For the complex representations
+// up to NF = 6 and the real NF = 3 (the register budget of the four U A_k and
+// B_k); the other representations keep k_force_hop.  (Four lanes per link, one
+// term each, was measured too: 100 registers and twice the resident warps, but
+// three times the instructions, each lane projecting its own partial sums,
+// and 1.6x slower at 16^4 NF = 6.)
+struct ProjTabK {
+  const int *off, *A;
+  const double2 *c;
+  int dimg;
+};
+
+template <int N, bool REAL>
+__global__ void __launch_bounds__(128) k_force_hop_w(double *fsum, const void *U, const double2 *X,
+                                                      const double2 *Y, Geo g, ProjTabK P, double coeff) {
+  extern __shared__ double hs[];  // [dimg][128]: this thread's generator sums in column tid
+  const int tid = threadIdx.x;
+  const long d = (long)blockIdx.x * 128 + tid;
+  const int mu = blockIdx.y;
+  if (d >= 2L * g.ld) return;
+  const int p = d >= g.ld ? 1 : 0;
+  if (d - p * g.ld >= g.VH) return;
+  for (int A = 0; A < P.dimg; A++) hs[A * 128 + tid] = 0.0;
+  int t, x, y, z;
+  dev_coords(g, (int)d, t, x, y, z);
+  const long dy = nbr_index(g, t, x, y, z, mu, +1);
+  const long lp = 2L * g.ld;
+  // A_k at x+mu: k = 0, 1 from Y (pairing X at x), k = 2, 3 from X (pairing Y at x)
+  double2 a[4][N];
+#pragma unroll
+  for (int pr = 0; pr < 2; pr++) {
+    const double2 *c2 = pr ? X : Y;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+      const double2 a0 = *sp_at(c2, dy, i, g.ld, N), a1 = *sp_at(c2, dy, N + i, g.ld, N);
+      const double2 a2 = *sp_at(c2, dy, 2 * N + i, g.ld, N), a3 = *sp_at(c2, dy, 3 * N + i, g.ld, N);
+      double2 &pt = a[2 * pr][i], &pt2 = a[2 * pr + 1][i];
+      if (mu == 0) { pt = cadd(a0, a2); pt2 = cadd(a1, a3); }
+      if (mu == 1) { pt = caddi(a0, a3); pt2 = caddi(a1, a2); }
+      if (mu == 2) { pt = cadd(a0, a3); pt2 = csub(a1, a2); }
+      if (mu == 3) { pt = caddi(a0, a2); pt2 = csubi(a1, a3); }
+    }
+  }
+  // U A_k, the link read once, row by row
+  double2 ua[4][N];
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) ua[k][i] = make_double2(0, 0);
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      const long idx = ((long)mu * N * N + i * N + j) * lp + d;
+      if (REAL) {
+        const double u = ((const double *)U)[idx];
+#pragma unroll
+        for (int k = 0; k < 4; k++) rmac(ua[k][i], u, a[k][j]);
+      } else {
+        const double2 u = ((const double2 *)U)[idx];
+#pragma unroll
+        for (int k = 0; k < 4; k++) cmac(ua[k][i], u, a[k][j]);
+      }
+    }
+  }
+  // B_k at x: k = 0, 1 from X, k = 2, 3 from Y (reusing a's registers)
+  double2 (&b)[4][N] = a;
+#pragma unroll
+  for (int pr = 0; pr < 2; pr++) {
+    const double2 *c1 = pr ? Y : X;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+      const double2 b0 = *sp_at(c1, d, i, g.ld, N), b1 = *sp_at(c1, d, N + i, g.ld, N);
+      const double2 b2 = *sp_at(c1, d, 2 * N + i, g.ld, N), b3 = *sp_at(c1, d, 3 * N + i, g.ld, N);
+      double2 &p2 = b[2 * pr][i], &p3 = b[2 * pr + 1][i];
+      if (mu == 0) { p2 = csub(b0, b2); p3 = csub(b1, b3); }
+      if (mu == 1) { p2 = csubi(b0, b3); p3 = csubi(b1, b2); }
+      if (mu == 2) { p2 = csub(b0, b3); p3 = cadd(b1, b2); }
+      if (mu == 3) { p2 = csubi(b0, b2); p3 = caddi(b1, b3); }
+    }
+  }
+  // s1_ij = sum_k (U A_k)_i conj(B_k)_j (real part only for real representations),
+  // projected element by element
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      double mr = 0.0, mi = 0.0;
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        mr += ua[k][i].x * b[k][j].x + ua[k][i].y * b[k][j].y;
+        if (!REAL) mi += ua[k][i].y * b[k][j].x - ua[k][i].x * b[k][j].y;
+      }
+      const int kk = i * N + j;
+      const int q1 = __ldg(P.off + kk + 1);
+      for (int q = __ldg(P.off + kk); q < q1; q++) {
+        const double2 c = __ldg(P.c + q);
+        hs[__ldg(P.A + q) * 128 + tid] += c.x * mr - c.y * mi;
+      }
+    }
+  }
+  for (int A = 0; A < P.dimg; A++) fsum[((long)mu * P.dimg + A) * lp + d] += coeff * hs[A * 128 + tid];
 }
 
 // g5 sigma_{mu nu} on a spinor held as [4][N] (force_fermion_core.c:123-250)
@@ -408,6 +523,16 @@ __global__ void k_force_logdet(double2 *clf, const double *idg, const double2 *i
     }
 }
 
+template <int N, bool REAL>
+static void launch_force_w(double *fsum, const void *U, const double2 *X, const double2 *Y, Geo g, ProjTabK P,
+                           double coeff, size_t smem) {
+  if constexpr ((!REAL && N <= 6) || (REAL && N == 3)) {
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(k_force_hop_w<N, REAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_force_hop_w<N, REAL><<<dim3(nb(2L * g.ld), 4), 128, smem, L.stream>>>(fsum, U, X, Y, g, P, coeff);
+  }
+}
+
 static ProjTab proj() {
   ProjTab P;
   P.off = L.d_proj_off;
@@ -489,7 +614,17 @@ int hrgpu_force_fermion_core(void *Xs, void *Ys, int auto_fill_odd, double dt, d
     HR_NF_DISPATCH(L.real, L.nf, (k_force_clover_fermion<N_, R_><<<dim3(nb(n), 6), 128, 0, L.stream>>>(L.cl_force, X, Y, g, residue)));
     HR_LAUNCH_CHECK();
   }
-  HR_NF_DISPATCH(L.real, L.nf, (k_force_hop<N_, R_><<<dim3(nb(n), 4), 128, 0, L.stream>>>(L.force_sum, L.U, X, Y, g, proj(), coeff)));
+  if ((!L.real && L.nf <= 6) || (L.real && L.nf == 3)) {
+    ProjTabK P;
+    P.off = L.d_projk_off;
+    P.A = L.d_projk_A;
+    P.c = L.d_projk_c;
+    P.dimg = L.dimg;
+    const size_t smem = sizeof(double) * 128 * L.dimg;
+    HR_NF_DISPATCH(L.real, L.nf, (launch_force_w<N_, R_>(L.force_sum, L.U, X, Y, g, P, coeff, smem)));
+  } else {
+    HR_NF_DISPATCH(L.real, L.nf, (k_force_hop<N_, R_><<<dim3(nb(n), 4), 128, 0, L.stream>>>(L.force_sum, L.U, X, Y, g, proj(), coeff)));
+  }
   HR_LAUNCH_CHECK();
   return 0;
 }

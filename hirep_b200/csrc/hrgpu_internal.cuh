@@ -96,6 +96,10 @@ struct Lattice {
   int *d_proj_off = nullptr;      // [dimg+1]
   int *d_proj_k = nullptr;
   double2 *d_proj_c = nullptr;    // conj(R(iT_A))_k / C(R)
+  // the same table by matrix element k: for each k the (A, coefficient) pairs
+  int *d_projk_off = nullptr;     // [nf*nf+1]
+  int *d_projk_A = nullptr;
+  double2 *d_projk_c = nullptr;
   double repr_norm2 = 0.0, fund_norm2 = 0.5;
   double *h_rT = nullptr;         // host copy of R(iT_A) as complex pairs [dimg][nf*nf][2]
   double *h_gT = nullptr;         // host copy of T_A [dimg][ng*ng][2]

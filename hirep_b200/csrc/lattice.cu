@@ -65,7 +65,7 @@ static void free_all() {
   cg_release();
   void *ptrs[] = {L.d_h2d, L.d_d2h, L.U, L.Uf, L.Ubf, L.Ug, L.mom, L.cl_term, L.cl_dg, L.cl_od, L.cl_idg, L.cl_iod,
                   L.cl_dg_f, L.cl_idg_f, L.cl_od_f, L.cl_iod_f, L.cl_ldet, L.force_sum, L.cl_force, L.d_proj_off,
-                  L.d_proj_k, L.d_proj_c, L.partials, L.d_scalars, L.tmp_o, L.tmp_e, L.tmp_e2, L.tmp_full,
+                  L.d_proj_k, L.d_proj_c, L.d_projk_off, L.d_projk_A, L.d_projk_c, L.partials, L.d_scalars, L.tmp_o, L.tmp_e, L.tmp_e2, L.tmp_full,
                   L.tmp_full2, L.tmp_o_f, L.tmp_e_f, L.tmp_full_f, L.stage, L.hop_err};
   for (void *p : ptrs) free_ptr(p);
   if (L.h_partials) cudaFreeHost(L.h_partials);
@@ -198,6 +198,24 @@ static int upload_projection_tables() {
   HR_CUDA(cudaMemcpy(L.d_proj_off, off.data(), sizeof(int) * (D + 1), cudaMemcpyHostToDevice));
   HR_CUDA(cudaMemcpy(L.d_proj_k, ks.data(), sizeof(int) * ks.size(), cudaMemcpyHostToDevice));
   HR_CUDA(cudaMemcpy(L.d_proj_c, cs.data(), sizeof(double2) * cs.size(), cudaMemcpyHostToDevice));
+  // inverted by matrix element k, for kernels that form one element at a time
+  std::vector<int> koff(F2 + 1, 0), kA;
+  std::vector<double2> kc;
+  for (int k = 0; k < F2; k++) {
+    for (int A = 0; A < D; A++)
+      if (std::abs(rT[A][k]) > 1e-14) {
+        cd c = std::conj(rT[A][k]) / rnorm;
+        kA.push_back(A);
+        kc.push_back(make_double2(c.real(), c.imag()));
+      }
+    koff[k + 1] = (int)kA.size();
+  }
+  HR_CUDA(cudaMalloc(&L.d_projk_off, sizeof(int) * (F2 + 1)));
+  HR_CUDA(cudaMalloc(&L.d_projk_A, sizeof(int) * kA.size()));
+  HR_CUDA(cudaMalloc(&L.d_projk_c, sizeof(double2) * kc.size()));
+  HR_CUDA(cudaMemcpy(L.d_projk_off, koff.data(), sizeof(int) * (F2 + 1), cudaMemcpyHostToDevice));
+  HR_CUDA(cudaMemcpy(L.d_projk_A, kA.data(), sizeof(int) * kA.size(), cudaMemcpyHostToDevice));
+  HR_CUDA(cudaMemcpy(L.d_projk_c, kc.data(), sizeof(double2) * kc.size(), cudaMemcpyHostToDevice));
   return 0;
 }
 
