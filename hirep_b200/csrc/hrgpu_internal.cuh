@@ -49,7 +49,7 @@ constexpr int MAXNF = 64;
 constexpr int RED_THREADS = 256;
 constexpr int RED_MAX_BLOCKS = 1184;  // 8 x 148 SMs
 constexpr int HOP_VARIANTS = 6;
-constexpr int HOPB_VARIANTS = 3;   // batch hopping kernel variants
+constexpr int HOPB_VARIANTS = 4;   // batch hopping kernel variants (3: tensor cores)
 constexpr int HOPB_MAXNB = 64;     // fields per batch
 
 struct Lattice {
@@ -123,6 +123,8 @@ struct Lattice {
   signed char hopb_variant[2][3][HOPB_MAXNB + 1] = {};
   float hopb_tune_ms[2][3][HOPB_MAXNB + 1][HOPB_VARIANTS] = {};
   int hopb_force = -1;
+  unsigned *hopb_err = nullptr;   // device error word of the tensor-core batch kernel
+  int num_sms = 0;                // multiprocessors of the device (persistent grids)
   // change counters: links (double and float are rewritten together) and the
   // packed clover blocks of each precision; copies made from them record these
   unsigned long gauge_gen = 0, clover_gen[2] = {0, 0};

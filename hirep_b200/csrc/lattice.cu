@@ -66,7 +66,7 @@ static void free_all() {
   void *ptrs[] = {L.d_h2d, L.d_d2h, L.U, L.Uf, L.Ubf, L.Ug, L.mom, L.cl_term, L.cl_dg, L.cl_od, L.cl_idg, L.cl_iod,
                   L.cl_dg_f, L.cl_idg_f, L.cl_od_f, L.cl_iod_f, L.cl_ldet, L.force_sum, L.cl_force, L.d_proj_off,
                   L.d_proj_k, L.d_proj_c, L.d_projk_off, L.d_projk_A, L.d_projk_c, L.partials, L.d_scalars, L.tmp_o, L.tmp_e, L.tmp_e2, L.tmp_full,
-                  L.tmp_full2, L.tmp_o_f, L.tmp_e_f, L.tmp_full_f, L.stage, L.hop_err};
+                  L.tmp_full2, L.tmp_o_f, L.tmp_e_f, L.tmp_full_f, L.stage, L.hop_err, L.hopb_err};
   for (void *p : ptrs) free_ptr(p);
   if (L.h_partials) cudaFreeHost(L.h_partials);
   delete[] L.h_h2d;
