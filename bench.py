@@ -240,7 +240,9 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 22-system solve (24^3x48 sextet)")
     ap.add_argument("--no-force", action="store_true", help="skip the force check (16^4 SU(4) antisymmetric)")
     ap.add_argument("--no-hmc", action="store_true", help="skip the HMC trajectory (32^3x64 SU(2) adjoint)")
+    ap.add_argument("--no-g5qmr", action="store_true", help="skip the HMC trajectory with HiRep's g5QMR force solves")
     ap.add_argument("--no-configs", action="store_true", help="skip the single-field operator at the other workloads")
+    ap.add_argument("--hmc-only", action="store_true", help="only the HMC trajectories (32^3x64 SU(2) adjoint)")
     ap.add_argument("--force-only", action="store_true",
                     help="only the force leg, without finite differences (for profiling its kernels)")
     ap.add_argument("--batch-op", default=None, metavar="TxXxYxZ",
@@ -269,6 +271,9 @@ def main():
         return batch_op_main(args, torch, G, F)
     if args.force_only:
         print(json.dumps({"force": run_force_check(torch, torch.cuda.current_stream(), G, F, fd=())}), flush=True)
+        return
+    if args.hmc_only:
+        print(json.dumps({"hmc": run_hmc_check(torch, G, F, g5qmr=not args.no_g5qmr)}), flush=True)
         return
     dist = None
     if world > 1:
@@ -405,7 +410,7 @@ def main():
     if world == 1 and not args.no_force:
         line["force"] = run_force_check(torch, stream, G, F)
     if world == 1 and not args.no_hmc:
-        line["hmc"] = run_hmc_check(torch, G, F)
+        line["hmc"] = run_hmc_check(torch, G, F, g5qmr=not args.no_g5qmr)
     if rank == 0 and world == 1 and not args.no_cpu:
         base, _ = cpu_reference_arm(args)
         line["cpu_baseline"] = base
@@ -653,7 +658,7 @@ def run_force_check(torch, stream, G, F, fd=((4, 1e-3), (4, 1e-4), (32, 1e-5))):
 H_DIMS, H_NG, H_BETA, H_MASS, H_EPS, H_SEED = (64, 32, 32, 32), 2, 2.25, -1.0, 0.2, 99
 
 
-def run_hmc_check(torch, G, F):
+def run_hmc_check(torch, G, F, g5qmr=True):
     """One trajectory with mixed-precision force solves against the same trajectory
     (same random numbers) with plain FP64 force solves.  Each form first runs an
     untimed 2-step warm-up trajectory (kernel autotuning, CUDA-graph capture,
@@ -684,6 +689,20 @@ def run_hmc_check(torch, G, F):
                      "plaquette_start": plaq0, "plaquette_end": lat.avr_plaquette()}
     out["speedup_mixed_vs_fp64"] = out["fp64"]["seconds"] / out["mixed"]["seconds"]
     out["dH_difference"] = out["mixed"]["dH"] - out["fp64"]["dH"]
+    if g5qmr:
+        # HiRep's own formulation of the same force solves (force_hmc.c:122-155): two
+        # g5QMR solves on D per force from the chronological MRE guess over 4 past
+        # solutions, and HiRep's g5QMR accept/reject solve on D
+        lat.set_gauge(u0)
+        lat.represent_gauge_field(True)
+        hmc = HMC(lat, H_BETA, H_MASS, tau=1.0, nsteps=20, force_err2=1e-20, mt_err2=1e-28, force_solver="g5qmr",
+                  draws="device", mre_past=4, mt_solver="g5qmr")
+        torch.cuda.synchronize()
+        r = hmc.trajectory(np.random.default_rng(H_SEED), metropolis=False)
+        out["g5qmr_mre4"] = {"seconds": r["seconds"], "dH": r["dH"], "force_solve_mvm": r["force_solve_iters"],
+                             "accept_reject_mvm": r["mt_iters"],
+                             "note": "HiRep's own force formulation: two g5QMR solves on D from the MRE guess; "
+                                     "MVM = D applications"}
     return out
 
 

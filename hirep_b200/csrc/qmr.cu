@@ -2,11 +2,13 @@
 // (LibHR/Inverters/MINRES.c) and the chronological initial guess MRE
 // (LibHR/Update/mre.c) on the device.
 //
-// The recursions are HiRep's, step for step; the fields live on the device and
-// every vector operation is a library kernel, while the handful of scalars per
-// iteration (alpha, rho, delta, the Givens rotations of every shift) are kept
-// on the host, which reads three reductions per g5QMR iteration.  These solvers
-// are HiRep's choice for the non-hermitian D (force_hmc.c:122-155,
+// The recursions are HiRep's.  g5QMR keeps every scalar on the device (alpha,
+// rho, delta, beta and the Givens rotations of every shift live in a state
+// struct; one-block folds update them from the partial sums of the fused
+// vector kernels), so an iteration is the operator plus five kernels and the
+// host reads the state once per chunk of iterations, as the CG does (cg.cu).
+// MINRES and MRE keep their few scalars on the host.  These solvers are
+// HiRep's choice for the non-hermitian D (force_hmc.c:122-155,
 // calc_prop.c:210-289) and the fallbacks around it.
 #include <math.h>
 #include <string.h>
@@ -46,9 +48,12 @@ static int qpool(int n, size_t bytes) {
   return 0;
 }
 
+static void qmr_release_state();
+
 void qmr_release() {
   for (void *p : QP.f) cudaFree(p);
   QP = QPool();
+  qmr_release_state();
 }
 
 // small wrappers over the linear algebra (FP64, parity par)
@@ -75,105 +80,306 @@ struct QLA {
   }
 };
 
-// plane rotation (c, s) with [c s; -s c] (a, b)^T = (1/r, 0)^T  (g5QMR_mshift.c:30-37)
-static void givens(double *r, double *c, double *s, double a, double b) {
-  if (fabs(a) < 1.e-15) {
-    *r = 1. / b;
-    *c = 0.;
-    *s = 1.;
-  } else {
-    const double t = b / a;
-    *c = 1. / sqrt(1. + t * t);
-    *s = t * (*c);
-    *r = 1. / ((*c) * a + (*s) * b);
+// ---------------------------------------------------------------------------
+// g5QMR_mshift_core (g5QMR_mshift.c:83-279) with the scalars on the device.
+// One iteration (p1, p2, Mp the three rotating directions, q1/q2 per shift):
+//   Mp = M p2 - s_0 p2                      operator + k_q_alpha (<g5 p2, Mp> partials)
+//   alpha = <g5 p2, Mp> / delta              k_q_fold_alpha
+//   Mp -= beta p1 + alpha p2                 k_q_p (|Mp|^2 and <g5 Mp, Mp> partials)
+//   rho, the Givens step of every shift,     k_q_fold_rho (one thread, HiRep's order;
+//   delta = <g5 Mp, Mp>/rho^2, beta, flags    the convergence and failure tests)
+//   per shift: q_new = d (p1 - t q1 - e q2),  k_q_shift (q_new overwrites q1 in place
+//   out += c2 r q_new; p2 = Mp / rho           and the two q buffers swap roles)
+// ---------------------------------------------------------------------------
+constexpr int QMAX = 64;
+constexpr int QMR_CHUNK = 4;  // iterations launched between two reads of the state
+
+struct QMRState {
+  double alpha, beta, delta, rho, scale, innorm2, err2;
+  int n, iter, max_iter, state, notconv;
+  double shift[QMAX], r[QMAX], s1[QMAX], s2[QMAX], c1[QMAX], c2[QMAX];
+  double t[QMAX], e[QMAX], d[QMAX], cout[QMAX];  // this iteration's coefficients per shift
+  int flag[QMAX], act[QMAX], qsel[QMAX], qpar[QMAX];
+};
+
+__device__ double q_fold(const double *partials, int nblocks, int stride, int off) {
+  double v = 0;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v += partials[(long)b * stride + off];
+  return block_sum(v);
+}
+
+__device__ __forceinline__ double q_g5(long e, int ld, int nf) {
+  return ((int)((e / ld) % (4 * nf)) / nf) < 2 ? 1.0 : -1.0;
+}
+
+// Mp -= s_0 p2 (the shift of the first system, g5QMR_mshift.c:128); partials of <g5 p2, Mp>
+__global__ void __launch_bounds__(RED_THREADS) k_q_alpha(const QMRState *S, double2 *Mp, const double2 *p2, long n,
+                                                         int ld, int nf, double *partials) {
+  if (S->state != 0) return;
+  const double s0 = S->shift[0];
+  double acc = 0.0;
+  const long stride = (long)gridDim.x * blockDim.x;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
+    const double2 a = p2[e];
+    double2 v = Mp[e];
+    rmac(v, -s0, a);
+    Mp[e] = v;
+    acc += q_g5(e, ld, nf) * (a.x * v.x + a.y * v.y);
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+
+__global__ void k_q_fold_alpha(QMRState *S, const double *partials, int nblocks) {
+  if (S->state != 0) return;
+  const double a = q_fold(partials, nblocks, 1, 0);
+  if (threadIdx.x == 0) S->alpha = a / S->delta;
+}
+
+// Mp -= beta p1 + alpha p2 (g5QMR_mshift.c:131-132); partials of |Mp|^2 and <g5 Mp, Mp>
+__global__ void __launch_bounds__(RED_THREADS) k_q_p(const QMRState *S, double2 *Mp, const double2 *p1,
+                                                     const double2 *p2, long n, int ld, int nf, double *partials) {
+  if (S->state != 0) return;
+  const double beta = S->beta, alpha = S->alpha;
+  double nrm = 0.0, g5n = 0.0;
+  const long stride = (long)gridDim.x * blockDim.x;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
+    double2 v = Mp[e];
+    rmac(v, -beta, p1[e]);
+    rmac(v, -alpha, p2[e]);
+    Mp[e] = v;
+    const double q = v.x * v.x + v.y * v.y;
+    nrm += q;
+    g5n += q_g5(e, ld, nf) * q;
+  }
+  nrm = block_sum(nrm);
+  g5n = block_sum(g5n);
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = nrm;
+    partials[2 * blockIdx.x + 1] = g5n;
   }
 }
 
-// g5QMR_mshift_core (g5QMR_mshift.c:83-279).  valid[i]: the true residual of
-// shift i is below err2.  Returns the MVM count in *iters.
+// rho, the Givens step of every shift, delta and beta, convergence (g5QMR_mshift.c:135-228)
+__global__ void k_q_fold_rho(QMRState *S, const double *partials, int nblocks) {
+  if (S->state != 0) return;
+  const double nrm = q_fold(partials, nblocks, 2, 0);
+  const double g5n = q_fold(partials, nblocks, 2, 1);
+  if (threadIdx.x != 0) return;
+  const int iter = ++S->iter;
+  const double rho = sqrt(nrm), alpha = S->alpha;
+  double beta = S->beta, maxm = 1.e-10;
+  int notconv = S->notconv;
+  S->rho = rho;
+  for (int i = 0; i < S->n; i++) {
+    S->act[i] = S->flag[i];
+    if (!S->flag[i]) continue;
+    const double a = alpha - S->shift[i] + S->shift[0];
+    const double t = S->s1[i] * beta;
+    const double e = S->c2[i] * S->c1[i] * beta + S->s2[i] * a;
+    const double m = S->c2[i] * a - S->s2[i] * S->c1[i] * beta;
+    S->s1[i] = S->s2[i];
+    S->c1[i] = S->c2[i];
+    double d, c, sn;
+    if (fabs(m) < 1.e-15) {  // the plane rotation of g5QMR_mshift.c:30-37
+      d = 1. / rho;
+      c = 0.;
+      sn = 1.;
+    } else {
+      const double tt = rho / m;
+      c = 1. / sqrt(1. + tt * tt);
+      sn = tt * c;
+      d = 1. / (c * m + sn * rho);
+    }
+    S->c2[i] = c;
+    S->s2[i] = sn;
+    if (fabs(m) > maxm) maxm = fabs(m);
+    S->t[i] = t;
+    S->e[i] = e;
+    S->d[i] = d;
+    S->cout[i] = c * S->r[i];
+    S->r[i] *= -sn;
+    S->qsel[i] = S->qpar[i];
+    S->qpar[i] ^= 1;
+    if (fabs(S->r[i] * S->r[i]) * (double)(1 + iter) < S->err2 * S->innorm2) {
+      S->flag[i] = 0;
+      --notconv;
+    }
+  }
+  S->scale = 0.0;
+  if (fabs(rho) > 1.e-13) {
+    S->scale = 1. / rho;
+    const double olddelta = S->delta;
+    S->delta = g5n / (rho * rho);
+    if (fabs(S->delta) < 1.e-6 || maxm < 1.e-3) notconv = 0;  // the method has failed
+    beta = rho * S->delta / olddelta;
+  } else {
+    notconv = 0;  // converged
+  }
+  S->beta = beta;
+  S->notconv = notconv;
+  if (notconv == 0 || (S->max_iter != 0 && iter >= S->max_iter)) S->state = 1;
+}
+
+// per shift: q_new = d (p1 - t q1 - e q2) into q1's buffer, out += c2 r q_new
+// (g5QMR_mshift.c:152-170); then p2 = Mp / rho (:188)
+__global__ void k_q_shift(const QMRState *S, double2 *const *out, double2 *const *qa, double2 *const *qb,
+                          const double2 *p1, double2 *p2, long n) {
+  if (S->state >= 2) return;
+  const int ns = S->n;
+  const double scale = S->scale;
+  const long stride = (long)gridDim.x * blockDim.x;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
+    const double2 pv = p1[e];
+    for (int i = 0; i < ns; i++) {
+      if (!S->act[i]) continue;
+      double2 *q1 = S->qsel[i] ? qb[i] : qa[i];
+      const double2 *q2 = S->qsel[i] ? qa[i] : qb[i];
+      const double d = S->d[i];
+      double2 v;
+      const double2 a = q1[e], b = q2[e];
+      v.x = (-S->t[i] * d) * a.x;
+      v.y = (-S->t[i] * d) * a.y;
+      rmac(v, -S->e[i] * d, b);
+      rmac(v, d, pv);
+      q1[e] = v;
+      double2 o = out[i][e];
+      rmac(o, S->cout[i], v);
+      out[i][e] = o;
+    }
+    if (scale != 0.0) {
+      double2 v = p2[e];
+      v.x *= scale;
+      v.y *= scale;
+      p2[e] = v;
+    }
+  }
+}
+
+__global__ void k_q_advance(QMRState *S) {
+  if (S->state == 1) S->state = 2;
+}
+
+struct QMRWork {
+  QMRState *S = nullptr, *hS = nullptr;
+  void **d_ptrs = nullptr;  // out[QMAX], qa[QMAX], qb[QMAX]
+};
+static QMRWork QW;
+
+static void qmr_release_state() {
+  if (QW.S) cudaFree(QW.S);
+  if (QW.hS) cudaFreeHost(QW.hS);
+  if (QW.d_ptrs) cudaFree(QW.d_ptrs);
+  QW = QMRWork();
+}
+
+// valid[i]: the true residual of shift i is below err2.  Returns the MVM count in *iters.
 static int g5qmr_core(short *valid, int op, double mass, int n, const double *shift, double err2, int max_iter,
                       const void *in, void *const *out, int *iters) {
   const int par = op_parity(op);
   const QLA la{par};
+  HR_REQUIRE(n >= 1 && n <= QMAX, HRGPU_E_ARG, "g5QMR: %d shifts (1..%d)", n, QMAX);
   QTRY(qpool(2 * n + 3, spinor_bytes(par, HRGPU_DOUBLE)));
-  std::vector<void *> q1(n), q2(n);
-  for (int i = 0; i < n; i++) {
-    q1[i] = QP.f[i];
-    q2[i] = QP.f[n + i];
+  if (!QW.S) {
+    HR_CUDA(cudaMalloc(&QW.S, sizeof(QMRState)));
+    HR_CUDA(cudaMallocHost(&QW.hS, sizeof(QMRState)));
+    HR_CUDA(cudaMalloc(&QW.d_ptrs, sizeof(void *) * 3 * QMAX));
   }
-  void *p1 = QP.f[2 * n], *p2 = QP.f[2 * n + 1], *Mp = QP.f[2 * n + 2], *tmp;
-  std::vector<double> r(n), s1(n), s2(n), c1(n), c2(n);
-  std::vector<short> flags(n, 1);
-  int cgiter = 0, notconverged = n;
+  void *P[3] = {QP.f[2 * n], QP.f[2 * n + 1], QP.f[2 * n + 2]};  // p1, p2, Mp
+  int ip1 = 0, ip2 = 1, imp = 2;
+  int cgiter = 0;
   double innorm2, rho, delta;
-  QTRY(la.op(LA_COPY, p2, in));
+  QTRY(la.op(LA_COPY, P[ip2], in));
   QTRY(la.sqnorm(in, &innorm2));
   if (n == 1) {  // out[0] is the start vector
-    QTRY(apply_op(op, HRGPU_DOUBLE, mass, Mp, out[0]));
-    QTRY(la.op(LA_MUL_ADD_ASSIGN, Mp, out[0], nullptr, -shift[0]));
-    QTRY(la.op(LA_SUB, p2, p2, Mp));
+    QTRY(apply_op(op, HRGPU_DOUBLE, mass, P[imp], out[0]));
+    QTRY(la.op(LA_MUL_ADD_ASSIGN, P[imp], out[0], nullptr, -shift[0]));
+    QTRY(la.op(LA_SUB, P[ip2], P[ip2], P[imp]));
   }
-  QTRY(la.sqnorm(p2, &rho));
+  QTRY(la.sqnorm(P[ip2], &rho));
   rho = sqrt(rho);
-  QTRY(la.op(LA_MUL, p2, p2, nullptr, 1. / rho));
-  QTRY(la.op(LA_ZERO, p1));
+  QTRY(la.op(LA_MUL, P[ip2], P[ip2], nullptr, 1. / rho));
+  QTRY(la.op(LA_ZERO, P[ip1]));
   for (int i = 0; i < n; i++) {
-    r[i] = rho;
-    c2[i] = c1[i] = 1.;
-    s1[i] = s2[i] = 0.;
     if (n != 1) QTRY(la.op(LA_ZERO, out[i]));
-    QTRY(la.op(LA_ZERO, q1[i]));
-    QTRY(la.op(LA_ZERO, q2[i]));
+    QTRY(la.op(LA_ZERO, QP.f[i]));
+    QTRY(la.op(LA_ZERO, QP.f[n + i]));
   }
-  QTRY(la.g5re(p2, p2, &delta));
+  QTRY(la.g5re(P[ip2], P[ip2], &delta));
   HR_REQUIRE(fabs(delta) >= 1.e-28, HRGPU_E_ARG,
              "g5QMR: gamma_5 norm of the initial guess is zero, change the initial guess");
-  double beta = delta;
-  do {
-    ++cgiter;
-    QTRY(apply_op(op, HRGPU_DOUBLE, mass, Mp, p2));
-    QTRY(la.op(LA_MUL_ADD_ASSIGN, Mp, p2, nullptr, -shift[0]));
-    double alpha;
-    QTRY(la.g5re(p2, Mp, &alpha));
-    alpha /= delta;
-    QTRY(la.op(LA_MUL_ADD_ASSIGN, Mp, p1, nullptr, -beta));
-    QTRY(la.op(LA_MUL_ADD_ASSIGN, Mp, p2, nullptr, -alpha));
-    tmp = p1; p1 = p2; p2 = Mp; Mp = tmp;
-    QTRY(la.sqnorm(p2, &rho));
-    rho = sqrt(rho);
-    double maxm = 1.e-10;
-    for (int i = 0; i < n; i++) {
-      if (!flags[i]) continue;
-      const double a = alpha - shift[i] + shift[0];
-      const double t = s1[i] * beta;
-      const double e = c2[i] * c1[i] * beta + s2[i] * a;
-      const double m = c2[i] * a - s2[i] * c1[i] * beta;
-      double d;
-      s1[i] = s2[i];
-      c1[i] = c2[i];
-      givens(&d, &c2[i], &s2[i], m, rho);
-      if (fabs(m) > maxm) maxm = fabs(m);
-      // new direction d (p1 - t q1 - e q2), then the rotation q1 <- q2 <- new
-      QTRY(la.op(LA_LC, Mp, q1[i], q2[i], -t * d, -e * d));
-      QTRY(la.op(LA_MUL_ADD_ASSIGN, Mp, p1, nullptr, d));
-      tmp = q1[i]; q1[i] = q2[i]; q2[i] = Mp; Mp = tmp;
-      QTRY(la.op(LA_MUL_ADD_ASSIGN, out[i], q2[i], nullptr, c2[i] * r[i]));
-      r[i] *= -s2[i];
-      if (fabs(r[i] * r[i]) * (double)(1 + cgiter) < err2 * innorm2) {
-        flags[i] = 0;
-        --notconverged;
-      }
+  QMRState &h = *QW.hS;
+  memset(&h, 0, sizeof(QMRState));
+  h.alpha = 0;
+  h.beta = delta;
+  h.delta = delta;
+  h.innorm2 = innorm2;
+  h.err2 = err2;
+  h.n = n;
+  h.max_iter = max_iter;
+  h.notconv = n;
+  for (int i = 0; i < n; i++) {
+    h.shift[i] = shift[i];
+    h.r[i] = rho;
+    h.c1[i] = h.c2[i] = 1.;
+    h.s1[i] = h.s2[i] = 0.;
+    h.flag[i] = 1;
+  }
+  HR_CUDA(cudaMemcpyAsync(QW.S, &h, sizeof(QMRState), cudaMemcpyHostToDevice, L.stream));
+  void *ptrs[3 * QMAX];
+  for (int i = 0; i < n; i++) {
+    ptrs[i] = out[i];
+    ptrs[QMAX + i] = QP.f[i];
+    ptrs[2 * QMAX + i] = QP.f[n + i];
+  }
+  HR_CUDA(cudaMemcpyAsync(QW.d_ptrs, ptrs, sizeof(void *) * 3 * QMAX, cudaMemcpyHostToDevice, L.stream));
+  double2 *const *d_out = (double2 *const *)QW.d_ptrs;
+  double2 *const *d_qa = (double2 *const *)(QW.d_ptrs + QMAX);
+  double2 *const *d_qb = (double2 *const *)(QW.d_ptrs + 2 * QMAX);
+  const long ne = (long)spinor_elems(par);
+  long gb = (ne + RED_THREADS - 1) / RED_THREADS;
+  const unsigned g = (unsigned)(gb < RED_MAX_BLOCKS ? gb : RED_MAX_BLOCKS);
+  const unsigned long m0 = mvm_count();
+  unsigned long per_it = 0;
+  int rc = 0;
+  L.cur_stop = &QW.S->state;
+  for (;;) {
+    for (int c = 0; c < QMR_CHUNK && !rc; c++) {
+      const unsigned long mb = mvm_count();
+      rc = apply_op(op, HRGPU_DOUBLE, mass, P[imp], P[ip2]);
+      if (rc) break;
+      per_it = mvm_count() - mb;
+      k_q_alpha<<<g, RED_THREADS, 0, L.stream>>>(QW.S, (double2 *)P[imp], (const double2 *)P[ip2], ne, L.ld, L.nf,
+                                                 L.partials);
+      k_q_fold_alpha<<<1, RED_THREADS, 0, L.stream>>>(QW.S, L.partials, g);
+      k_q_p<<<g, RED_THREADS, 0, L.stream>>>(QW.S, (double2 *)P[imp], (const double2 *)P[ip1],
+                                             (const double2 *)P[ip2], ne, L.ld, L.nf, L.partials);
+      k_q_fold_rho<<<1, RED_THREADS, 0, L.stream>>>(QW.S, L.partials, g);
+      // the three directions rotate: p1 <- p2, p2 <- Mp, Mp <- p1
+      const int o1 = ip1;
+      ip1 = ip2;
+      ip2 = imp;
+      imp = o1;
+      k_q_shift<<<g, RED_THREADS, 0, L.stream>>>(QW.S, d_out, d_qa, d_qb, (const double2 *)P[ip1], (double2 *)P[ip2],
+                                                 ne);
+      k_q_advance<<<1, 1, 0, L.stream>>>(QW.S);
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) rc = fail_cuda(e, "g5QMR iteration", __FILE__, __LINE__);
     }
-    if (fabs(rho) > 1.e-13) {
-      QTRY(la.op(LA_MUL, p2, p2, nullptr, 1. / rho));
-      const double olddelta = delta;
-      QTRY(la.g5re(p2, p2, &delta));
-      if (fabs(delta) < 1.e-6 || maxm < 1.e-3) notconverged = 0;  // the method has failed
-      beta = rho * delta / olddelta;
-    } else {
-      notconverged = 0;  // converged
+    if (rc) break;
+    cudaError_t e = cudaMemcpyAsync(&h, QW.S, sizeof(QMRState), cudaMemcpyDeviceToHost, L.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(L.stream);
+    if (e != cudaSuccess) {
+      rc = fail_cuda(e, "g5QMR state readback", __FILE__, __LINE__);
+      break;
     }
-  } while ((max_iter == 0 || cgiter < max_iter) && notconverged);
+    if (h.state != 0) break;
+  }
+  L.cur_stop = nullptr;
+  if (rc) return rc;
+  mvm_restore(m0 + (unsigned long)h.iter * per_it);  // the launches after convergence did nothing
+  cgiter = h.iter;
+  void *Mp = P[imp];
   for (int i = 0; i < n; i++) {
     QTRY(apply_op(op, HRGPU_DOUBLE, mass, Mp, out[i]));
     ++cgiter;
