@@ -295,3 +295,55 @@ class HiRep:
         self._slot(0, par)
         self._put(0, 0, inp, par)
         return float(self.cmd("sqnorm 0 0"))
+
+    # g5QMR, MINRES -----------------------------------------------------------
+    def g5QMR_mshift(self, name, m, shifts, err2, inp, par, max_iter=0, guess=None):
+        """g5QMR_mshift (g5QMR_mshift.c:481-542) on (M - shifts[i]), M = NAME(m), the
+        gamma_5-hermitian Dirac operator.  Returns (out, MVM)."""
+        n = len(shifts)
+        self._slot(2, par)
+        self._slot(3, par, n)
+        self._put(2, 0, inp, par)
+        for k in range(n):
+            if k == 0 and guess is not None:
+                self._put(3, 0, guess, par)
+            else:
+                self._put(3, k, np.zeros((self.nsites(par), 4, self.nf)), par)
+        sh = " ".join(repr(float(s)) for s in shifts)
+        mvm = int(self.cmd(f"g5qmr {name} {float(m)!r} {float(err2)!r} {int(max_iter)} 2 3 {n} {sh}"))
+        return np.stack([self._get(3, k, par) for k in range(n)]), mvm
+
+    def MINRES(self, name, m, err2, inp, par, max_iter=0):
+        """MINRES (MINRES.c:160-172) on the hermitian NAME(m), no trial vector."""
+        self._slot(2, par)
+        self._slot(3, par)
+        self._put(2, 0, inp, par)
+        self._put(3, 0, np.zeros((self.nsites(par), 4, self.nf)), par)
+        mvm = int(self.cmd(f"minres {name} {float(m)!r} {float(err2)!r} {int(max_iter)} 2 3"))
+        return self._get(3, 0, par), mvm
+
+    # HMC pieces and IO --------------------------------------------------------
+    def momenta_set(self, mom):
+        mom = np.ascontiguousarray(mom, np.float64)
+        assert mom.shape == (self.V, 4, self.dimg)
+        mom.tofile(self._path("mom.bin"))
+        self.cmd(f"mom_load {self._path('mom.bin')}")
+
+    def momenta_get(self):
+        self.cmd(f"mom_save {self._path('mom.bin')}")
+        return np.fromfile(self._path("mom.bin"), np.float64).reshape(self.V, 4, self.dimg)
+
+    def force0(self, dt, beta):
+        """force0 (force0.c:22-99, plaquette action): momenta += -dt beta/NG proj(U staples^+)."""
+        self.cmd(f"force0 {float(dt)!r} {float(beta)!r}")
+
+    def update_gauge_field(self, dt):
+        """update_gauge_field (field_update.c:18-66): U <- ExpX(dt, momenta) U, every 17th
+        call reunitarised, then represent_gauge_field."""
+        self.cmd(f"update_gauge {float(dt)!r}")
+
+    def write_gauge_field(self, path):
+        self.cmd(f"gauge_write {path}")
+
+    def read_gauge_field(self, path):
+        self.cmd(f"gauge_read {path}")

@@ -45,6 +45,12 @@
  *   time NAME M OUT IN W R   W warm-up and R timed applications, reply
  *                            "ok MEDIAN_US MIN_US THREADS"
  *   timecg NAME M ERR2 IN OUT W R   the same for a single-shift cg_mshift
+ *   g5qmr NAME M ERR2 MAXIT IN OUT N s1..sN   g5QMR_mshift, reply "ok MVM"
+ *   minres NAME M ERR2 MAXIT IN OUT           MINRES (no trial), reply "ok MVM"
+ *   mom_load PATH / mom_save PATH             the momenta field [V][4][NG*NG-1]
+ *   force0 DT BETA           force0 (the plaquette action's force) into the momenta
+ *   update_gauge DT          update_gauge_field: U <- exp(dt mom) U, represented
+ *   gauge_write PATH / gauge_read PATH        write_gauge_field / read_gauge_field (+ represent)
  *   quit
  */
 #define MAIN_PROGRAM
@@ -81,6 +87,7 @@
 
 #define NSLOT 64
 static spinor_field *slot[NSLOT];
+static suNg_av_field *g_mom = NULL;
 static int slot_n[NSLOT];
 static FILE *reply;
 
@@ -401,6 +408,99 @@ static void run(char *line)
     say("ok %.3f %.3f %d %d", t[r / 2], t[0], threads(), mvm);
     free(t);
     return;
+  }
+  if (strcmp(cmd, "g5qmr") == 0 || strcmp(cmd, "minres") == 0)
+  {
+    double err2;
+    int maxit, in, out, off = 0;
+    int qmr = cmd[0] == 'g';
+    if (qmr)
+    {
+      if (sscanf(line, "%*s %63s %lf %lf %d %d %d %d%n", d, &m, &err2, &maxit, &in, &out, &n, &off) != 7)
+        return say("err g5qmr args");
+    }
+    else
+    {
+      if (sscanf(line, "%*s %63s %lf %lf %d %d %d", d, &m, &err2, &maxit, &in, &out) != 6)
+        return say("err minres args");
+      n = 1;
+    }
+    int id = find_op(d);
+    if (id < 0 || n < 1 || n > 64 || !field_of(in, 0) || !field_of(out, n - 1))
+      return say("err %s operator or slot", cmd);
+    cur_f = ops[id].f;
+    cur_m = m;
+    if (!qmr)
+    {
+      MINRES_par mp;
+      mp.err2 = err2;
+      mp.max_iter = maxit;
+      return say("ok %d", MINRES(&mp, cur_op, field_of(in, 0), field_of(out, 0), NULL));
+    }
+    double sh[64] = {0};
+    char *p = line + off;
+    for (int j = 0; j < n; j++)
+    {
+      int used;
+      if (sscanf(p, "%lf%n", &sh[j], &used) != 1)
+        return say("err g5qmr shifts");
+      p += used;
+    }
+    mshift_par par;
+    par.n = n;
+    par.shift = sh;
+    par.err2 = err2;
+    par.max_iter = maxit;
+    par.add_par = NULL;
+    return say("ok %d", g5QMR_mshift(&par, cur_op, field_of(in, 0), field_of(out, 0)));
+  }
+  if (strcmp(cmd, "mom_load") == 0 || strcmp(cmd, "mom_save") == 0)
+  {
+    if (sscanf(line, "%*s %511s", a) != 1)
+      return say("err");
+    if (!g_mom)
+      g_mom = alloc_avfield(&glattice);
+    return say(rw(a, g_mom->ptr, 4 * (size_t)glattice.gsize_gauge * sizeof(suNg_algebra_vector), cmd[4] == 's')
+                   ? "err io"
+                   : "ok");
+  }
+  if (strcmp(cmd, "force0") == 0)
+  {
+    double dt, beta;
+    if (sscanf(line, "%*s %lf %lf", &dt, &beta) != 2 || !g_mom)
+      return say("err force0");
+    force_gauge_par fp;
+    fp.beta = beta;
+    fp.c0 = 1.0;
+    fp.c1 = 0.0;
+    fp.momenta = &g_mom;
+    force0(dt, &fp);
+    return say("ok");
+  }
+  if (strcmp(cmd, "update_gauge") == 0)
+  {
+    double dt;
+    if (sscanf(line, "%*s %lf", &dt) != 1 || !g_mom)
+      return say("err update_gauge");
+    field_gauge_par gp;
+    gp.field = &u_gauge;
+    gp.momenta = &g_mom;
+    update_gauge_field(dt, &gp);
+    return say("ok");
+  }
+  if (strcmp(cmd, "gauge_write") == 0 || strcmp(cmd, "gauge_read") == 0)
+  {
+    if (sscanf(line, "%*s %511s", a) != 1)
+      return say("err");
+    if (cmd[6] == 'w')
+      write_gauge_field(a);
+    else
+    {
+      read_gauge_field(a);
+      start_gf_sendrecv(u_gauge);
+      represent_gauge_field();
+    }
+    return say("ok");
   }
   if (strcmp(cmd, "force") == 0)
   {

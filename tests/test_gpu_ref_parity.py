@@ -195,3 +195,80 @@ def test_config5_full_size_adjoint_is_hireps():
     fe, out = lat.field(G.EVEN, host=e), lat.field(G.EVEN)
     lat.Dphi_eopre(m, out, fe)
     assert rel(out.download(), want) < 1e-13
+
+
+# ---------------------------------------------------------------------------
+# the "next" rows against HiRep: g5QMR, the gauge force and link update, and
+# configuration files written and read by each side
+# ---------------------------------------------------------------------------
+def test_gpu_g5qmr_is_hireps():
+    """g5QMR_mshift on Dphi_eopre with three shifts, SU(3) fundamental 8x8x4x4:
+    MVM count within 5 % of HiRep's, solutions to 1e-8, true residuals below err2."""
+    need("su3_fund")
+    dims, m, shifts, err2 = (8, 8, 4, 4), 0.1, [0.0, -0.1, 0.05], 1e-26
+    u = F.smooth_gauge(7, 1024, 3, 0.3)
+    e = F.gaussian_spinor(5, 512, 3)
+    with H.HiRep("su3_fund", *dims) as h:
+        h.set_gauge(u)
+        xh, mvm_h = h.g5QMR_mshift("Dphi_eopre", m, shifts, err2, e, H.EVEN, max_iter=5000)
+    lat = lattice(dims, "su3_fund", u)
+    fb = lat.field(G.EVEN, host=e)
+    outs = [lat.field(G.EVEN) for _ in shifts]
+    it, ok = lat.g5QMR_mshift(G.OP_DPHI_EOPRE, m, shifts, err2, fb, outs, max_iter=5000)
+    assert ok
+    assert abs(it - mvm_h) <= max(3, mvm_h // 20), (it, mvm_h)
+    for k in range(len(shifts)):
+        assert rel(outs[k].download(), xh[k]) < 1e-8
+
+
+@pytest.mark.parametrize("cfg", ["su2_adj", "su4_asym"])
+def test_gpu_gauge_force_and_link_update_are_hireps(cfg):
+    """force0 into given momenta and update_gauge_field, against HiRep (builds whose
+    fundamental links carry no boundary sign)."""
+    need(cfg)
+    ng = H.CONFIGS[cfg][0]
+    dims = (4, 4, 4, 4)
+    u = F.smooth_gauge(9, 256, ng, 0.3)
+    mom = np.random.default_rng(42).standard_normal((256, 4, ng * ng - 1))
+    with H.HiRep(cfg, *dims) as h:
+        h.set_gauge(u)
+        h.momenta_set(mom)
+        h.force0(0.23, 2.25)
+        fh = h.momenta_get()
+        h.momenta_set(mom)
+        h.update_gauge_field(0.05)
+        uh = h.gauge()
+    lat = lattice(dims, cfg, u)
+    lat.momenta_set(mom)
+    lat.force0(0.23, 2.25)
+    assert rel(lat.momenta_get(), fh) < 1e-13
+    lat.momenta_set(mom)
+    lat.update_gauge_field(0.05)
+    assert rel(lat.gauge_get(), uh) < 1e-13
+
+
+@pytest.mark.parametrize("cfg", ["su2_adj", "su4_asym"])
+def test_gpu_configuration_files_are_hireps(cfg, tmp_path):
+    """HiRep's write_gauge_field read by the library, and the library's file read by
+    HiRep's read_gauge_field (SU(2): the quaternion format of archive_su2quat.c)."""
+    need(cfg)
+    ng = H.CONFIGS[cfg][0]
+    dims = (4, 4, 4, 6)
+    V = 4 * 4 * 4 * 6
+    u = F.smooth_gauge(13, V, ng, 0.4)
+    f_hirep, f_ours = tmp_path / "conf_hirep", tmp_path / "conf_ours"
+    lat = lattice(dims, cfg, u)
+    lat.write_gauge_field(f_ours)
+    with H.HiRep(cfg, *dims) as h:
+        h.set_gauge(u)
+        plaq_h = h.plaquette()
+        h.write_gauge_field(str(f_hirep))
+        h.read_gauge_field(str(f_ours))
+        u_from_ours = h.gauge()
+        plaq_from_ours = h.plaquette()
+    assert rel(u_from_ours, u) < 1e-14
+    assert abs(plaq_from_ours - plaq_h) < 1e-14
+    lat2 = lattice(dims, cfg, F.smooth_gauge(14, V, ng, 0.4))
+    pf, pr = lat2.read_gauge_field(f_hirep)
+    assert abs(pf - plaq_h) < 1e-14 and abs(pr - plaq_h) < 1e-13
+    assert rel(lat2.gauge_get(), u) < 1e-14

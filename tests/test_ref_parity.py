@@ -240,3 +240,54 @@ def test_config1_hot_start_from_hireps_ranlux():
     x_o, mvm_o = o.cg_mshift(O.OP_G5DPHI_SQ, [0.0], 1e-28, f, max_iter=5000)
     assert mvm_o == mvm_h
     assert rel(x_o[0], x_h[0]) < 1e-12
+
+
+# ---------------------------------------------------------------------------
+# the "next" rows: g5QMR and MINRES, the gauge force and the link update
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("cfg", ["su3_fund", "su4_asym", "su2_adj"])
+def test_g5qmr_is_hireps(cfg):
+    """g5QMR_mshift (g5QMR_mshift.c:481-542) on Dphi_eopre with three shifts: the
+    oracle's MVM count equals HiRep's, solutions to 1e-10 (the solver's accuracy)."""
+    h, o, _ = pair(cfg, (8, 8, 4, 4))
+    m, shifts, err2 = 0.1, [0.0, -0.1, 0.05], 1e-26
+    o.set_mass(m)
+    e = F.gaussian_spinor(5, o.VH, o.nf)
+    with h:
+        xh, mvm_h = h.g5QMR_mshift("Dphi_eopre", m, shifts, err2, e, H.EVEN, max_iter=5000)
+    xo, mvm_o = o.g5QMR_mshift(O.OP_DPHI_EOPRE, shifts, err2, e, max_iter=5000)
+    assert mvm_o == mvm_h
+    for k in range(len(shifts)):
+        assert rel(xo[k], xh[k]) < 1e-10
+
+
+def test_minres_is_hireps():
+    """MINRES (MINRES.c:160-172) on the hermitian g5Dphi_eopre."""
+    h, o, _ = pair("su3_fund", (8, 8, 4, 4))
+    m, err2 = 0.1, 1e-26
+    o.set_mass(m)
+    e = F.gaussian_spinor(6, o.VH, o.nf)
+    with h:
+        xh, mvm_h = h.MINRES("g5Dphi_eopre", m, err2, e, H.EVEN, max_iter=5000)
+    xo, mvm_o = o.MINRES(O.OP_G5DPHI_EOPRE, err2, e, max_iter=5000)
+    assert mvm_o == mvm_h
+    assert rel(xo, xh) < 1e-10
+
+
+@pytest.mark.parametrize("cfg", ["su3_fund", "su2_adj", "su4_asym"])
+def test_gauge_force_and_link_update_are_hireps(cfg):
+    """force0 (force0.c:22-99) into given momenta, and update_gauge_field
+    (field_update.c:18-66, ExpX), on the links HiRep holds (in a fundamental build
+    the antiperiodic sign sits on u_gauge itself)."""
+    h, o, _ = pair(cfg, (4, 4, 4, 4))
+    ng = H.CONFIGS[cfg][0]
+    rng = np.random.default_rng(41)
+    mom = rng.standard_normal((o.V, 4, ng * ng - 1))
+    with h:
+        uh = h.gauge()
+        h.momenta_set(mom)
+        h.force0(0.23, 2.25)
+        assert rel(h.momenta_get(), o.force0(0.23, 2.25, uh, mom)) < 1e-13
+        h.momenta_set(mom)
+        h.update_gauge_field(0.05)
+        assert rel(h.gauge(), o.update_gauge_field(0.05, uh, mom)) < 1e-13
