@@ -4,46 +4,65 @@
 #pragma once
 #include "dirac.cuh"
 #include "hop_tc.cuh"
+#include "hop_tcp.cuh"
 #include "hop_tile.cuh"
 
 namespace hrgpu {
 
+// Outside a stream capture the error word of a tensor-core launch is read back
+// at once, so a bounded wait that gave up is reported as an error status.
+inline int tc_check_error_word(const char *what) {
+  HR_LAUNCH_CHECK();
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  HR_CUDA(cudaStreamIsCapturing(L.stream, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return 0;
+  unsigned h = 0;
+  HR_CUDA(cudaMemcpyAsync(&h, L.hopb_err, sizeof(unsigned), cudaMemcpyDeviceToHost, L.stream));
+  HR_CUDA(cudaStreamSynchronize(L.stream));
+  if (h) {
+    HR_CUDA(cudaMemsetAsync(L.hopb_err, 0, sizeof(unsigned), L.stream));
+    set_error("%s: a bounded wait for its MMAs gave up (error word %u)", what, h);
+    return HRGPU_E_CUDA;
+  }
+  return 0;
+}
+
+inline int tc_prepare() {
+  if (!L.hopb_err) {
+    HR_CUDA(cudaMalloc(&L.hopb_err, sizeof(unsigned)));
+    HR_CUDA(cudaMemsetAsync(L.hopb_err, 0, sizeof(unsigned), L.stream));
+  }
+  if (!L.num_sms) {
+    int dev = 0;
+    HR_CUDA(cudaGetDevice(&dev));
+    HR_CUDA(cudaDeviceGetAttribute(&L.num_sms, cudaDevAttrMultiProcessorCount, dev));
+  }
+  return 0;
+}
+
 // variant 3: the tensor-core kernel (FP32, complex NF = 6, nb <= 32; -1 where
-// it is not built).  A persistent grid of up to four CTAs per SM; outside a
-// stream capture the launch's error word is read back at once, so a bounded
-// wait that gave up is reported as an error status.
+// it is not built), a persistent grid of up to four CTAs per SM.
+// variant 4: the same GEMM with the neighbours prefetched (nb <= 16), one CTA
+// of two warpgroups per SM.
 template <typename R, int EP>
-int launch_batch_tc(TileArgs<R> &a) {
+int launch_batch_tc(TileArgs<R> &a, int variant) {
   if constexpr (sizeof(R) != 4) {
     return -1;
   } else {
-    if (L.real || L.nf != 6 || a.nb > 32) return -1;
-    if (!L.hopb_err) {
-      HR_CUDA(cudaMalloc(&L.hopb_err, sizeof(unsigned)));
-      HR_CUDA(cudaMemsetAsync(L.hopb_err, 0, sizeof(unsigned), L.stream));
+    if (L.real || L.nf != 6 || a.nb > (variant == 4 ? TCP_NBMAX : 32)) return -1;
+    if (int rc = tc_prepare()) return rc;
+    if (variant == 3) {
+      const size_t smem = tc_smem_bytes<6>();
+      HR_CUDA(cudaFuncSetAttribute(k_hopt_tc<6, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      const long grid = std::min<long>(L.VH, 4L * L.num_sms);
+      k_hopt_tc<6, EP><<<(unsigned)grid, TC_THREADS, smem, L.stream>>>(a, L.hopb_err);
+      return tc_check_error_word("tensor-core batch kernel");
     }
-    if (!L.num_sms) {
-      int dev = 0;
-      HR_CUDA(cudaGetDevice(&dev));
-      HR_CUDA(cudaDeviceGetAttribute(&L.num_sms, cudaDevAttrMultiProcessorCount, dev));
-    }
-    const size_t smem = tc_smem_bytes<6>();
-    HR_CUDA(cudaFuncSetAttribute(k_hopt_tc<6, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const long grid = std::min<long>(L.VH, 4L * L.num_sms);
-    k_hopt_tc<6, EP><<<(unsigned)grid, TC_THREADS, smem, L.stream>>>(a, L.hopb_err);
-    HR_LAUNCH_CHECK();
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    HR_CUDA(cudaStreamIsCapturing(L.stream, &cs));
-    if (cs != cudaStreamCaptureStatusNone) return 0;
-    unsigned h = 0;
-    HR_CUDA(cudaMemcpyAsync(&h, L.hopb_err, sizeof(unsigned), cudaMemcpyDeviceToHost, L.stream));
-    HR_CUDA(cudaStreamSynchronize(L.stream));
-    if (h) {
-      HR_CUDA(cudaMemsetAsync(L.hopb_err, 0, sizeof(unsigned), L.stream));
-      set_error("tensor-core batch kernel: a bounded wait for its MMAs gave up (error word %u)", h);
-      return HRGPU_E_CUDA;
-    }
-    return 0;
+    const size_t smem = TcpLayout<6>::SMEM;
+    HR_CUDA(cudaFuncSetAttribute(k_hopt_tcp<6, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const long grid = std::min<long>(L.VH, (long)L.num_sms);
+    k_hopt_tcp<6, EP><<<(unsigned)grid, TCP_THREADS, smem, L.stream>>>(a, L.hopb_err);
+    return tc_check_error_word("tensor-core batch kernel (prefetched)");
   }
 }
 
@@ -51,7 +70,7 @@ int launch_batch_tc(TileArgs<R> &a) {
 template <typename R, int EP>
 int launch_batch_variant(TileArgs<R> &a, int variant) {
   a.g = make_geo();
-  if (variant == 3) return launch_batch_tc<R, EP>(a);
+  if (variant >= 3) return launch_batch_tc<R, EP>(a, variant);
   // 32 threads per (group of 8 sites, tile)
   const long threads = ((L.VH + TILE_S - 1) / TILE_S) * 32L * ((a.nb + TILE_F - 1) / TILE_F);
   dim3 grid((unsigned)((threads + HOPT_THREADS - 1) / HOPT_THREADS)), block(HOPT_THREADS);
@@ -113,7 +132,7 @@ int launch_batch(TileArgs<R> &a) {
     // the events are destroyed on every way out of the loop
     auto tune = [&]() -> int {
       for (int cand = 0; cand < HOPB_VARIANTS; cand++) {
-        if (cand == 3) {  // the tensor-core kernel runs when pinned (hrgpu_set_batch_variant(3))
+        if (cand >= 3) {  // the tensor-core kernels run when pinned (hrgpu_set_batch_variant(3 or 4))
           L.hopb_tune_ms[pi][EP][a.nb][cand] = -1.0f;
           continue;
         }

@@ -387,10 +387,12 @@ int hrgpu_apply_op_batch(int op, int prec, double mass, void *out, const void *i
 /* batch hopping kernel variants (0, 1, 2: one thread per site and field with
  * the register budget of 1, 3, 4 resident blocks per SM; 3: the link products
  * on the tensor cores, tcgen05 kind::tf32 with three products for FP32
- * accuracy, FP32 and complex NF = 6 only, nb <= 32, run only when pinned):
- * -1 (default) autotunes variants 0-2 per precision, epilogue and nb at first
- * use; hrgpu_batch_tuning reports the choice (-1: not tuned yet) and the
- * tuning times in ms (4 entries, -1 for a variant not timed). */
+ * accuracy, FP32 and complex NF = 6 only, nb <= 32; 4: the same with the
+ * neighbours prefetched into shared memory two sites ahead, nb <= 16; 3 and 4
+ * run only when pinned): -1 (default) autotunes variants 0-2 per precision,
+ * epilogue and nb at first use; hrgpu_batch_tuning reports the choice (-1: not
+ * tuned yet) and the tuning times in ms (5 entries, -1 for a variant not
+ * timed). */
 int hrgpu_set_batch_variant(int variant);
 int hrgpu_batch_tuning(int prec, int epilogue, int nb, int *chosen, float *ms);
 /* cg_mshift for many sources at once (op: g5Dphi_eopre_sq or g5Cphi_eopre_sq).

@@ -248,25 +248,25 @@ def test_batch_autotuner_reports_its_choice():
     bi, bo = lat.batch(nb), lat.batch(nb)
     lat.apply_op_batch(G.OP_G5CPHI_EOPRE, -0.2, bo, bi)
     chosen = ctypes.c_int(-2)
-    ms = (ctypes.c_float * 4)()
+    ms = (ctypes.c_float * 5)()
     for ep in (1, 2):  # the two clover epilogues ran
         G._check(lat.L.hrgpu_batch_tuning(G.DOUBLE, ep, nb, ctypes.byref(chosen), ms), "batch_tuning")
         assert 0 <= chosen.value < 3
-        assert all(t > 0 for t in ms[:3]) and ms[3] == -1.0  # the tensor-core variant runs only when pinned
+        assert all(t > 0 for t in ms[:3]) and ms[3] == ms[4] == -1.0  # the tensor-core variants run only when pinned
     G._check(lat.L.hrgpu_batch_tuning(G.FLOAT, 0, nb, ctypes.byref(chosen), ms), "batch_tuning")
     assert chosen.value == -1  # not tuned: never ran
 
 
-@pytest.mark.parametrize("nb", [5, 12, 32])
+@pytest.mark.parametrize("variant,nb", [(3, 5), (3, 12), (3, 32), (4, 5), (4, 12), (4, 16)])
 @pytest.mark.parametrize("ng,rep,clover", [(3, O.SYM, True), (4, O.ASYM, False)])
-def test_batch_tensor_core_variant(nb, ng, rep, clover):
-    """Variant 3, the link products on the tensor cores (tcgen05, kind::tf32, three
-    products for FP32 accuracy), for the NF = 6 representations: every field of
-    the FP32 batched operator against the FP32 single-field operator (2e-6, the
-    FP32 operators' tolerance) and against the oracle's FP64 operator; a batch
-    of more than 32 fields is refused for this variant."""
+def test_batch_tensor_core_variant(variant, nb, ng, rep, clover):
+    """Variants 3 and 4, the link products on the tensor cores (tcgen05, kind::tf32,
+    three products for FP32 accuracy), for the NF = 6 representations: every field
+    of the FP32 batched operator against the FP32 single-field operator (2e-6, the
+    FP32 operators' tolerance) and against the oracle's FP64 operator; a batch of
+    more than 32 (variant 3) or 16 (variant 4) fields is refused."""
     o, lat = setup((4, 4, 4, 8), ng, rep, seed=17, clover=1.0 if clover else None)
-    G._check(lat.L.hrgpu_set_batch_variant(3), "set_batch_variant")
+    G._check(lat.L.hrgpu_set_batch_variant(variant), "set_batch_variant")
     try:
         m = -0.3 if clover else -0.1
         ops = OPS_C[1:] if clover else OPS_W  # (the clover operators have FP32 forms with gamma_5)
@@ -278,12 +278,12 @@ def test_batch_tensor_core_variant(nb, ng, rep, clover):
         for op, name in ops:
             lat.apply_op_batch(op, m, bout, bin_)
             bout.unpack(outs)
-            for f in (0, nb // 2, nb - 1):
+            for f in sorted({0, nb // 2, nb - 1}):
                 getattr(lat, name + "_flt")(m, single, fs[f])
                 assert rel(outs[f].download(), single.download()) < 2e-6, (name, f)
                 assert rel(outs[f].download().astype(complex), getattr(o, name)(m, hs[f])) < 2e-6, (name, f)
-        if nb == 32:
-            big_in, big_out = lat.batch(33, G.FLOAT), lat.batch(33, G.FLOAT)
+        if nb == (32 if variant == 3 else 16):
+            big_in, big_out = lat.batch(nb + 1, G.FLOAT), lat.batch(nb + 1, G.FLOAT)
             with pytest.raises(G.HRGPUError, match="not built"):
                 lat.apply_op_batch(ops[0][0], m, big_out, big_in)
     finally:
