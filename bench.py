@@ -608,6 +608,13 @@ def run_force_check(torch, stream, G, F, fd=((4, 1e-3), (4, 1e-4), (32, 1e-5))):
     solve_s = time.time() - t0
     f64, _ = force()
     core_ms = float(np.median([force()[1] for _ in range(5)]))
+    by_variant = {}
+    for v in (1, 2, 3):  # the kernels of the hopping force (hrgpu_set_force_variant)
+        G._check(lat.L.hrgpu_set_force_variant(v), "set_force_variant")
+        fv, _ = force()
+        by_variant[str(v)] = {"ms": float(np.median([force()[1] for _ in range(5)])),
+                              "max_rel_diff_vs_default": float(np.abs(fv - f64).max() / np.abs(f64).max())}
+    G._check(lat.L.hrgpu_set_force_variant(0), "set_force_variant")
     solve(flt=True, err2=1e-26)
     f32, _ = force()
     rng = np.random.default_rng(32)
@@ -641,6 +648,9 @@ def run_force_check(torch, stream, G, F, fd=((4, 1e-3), (4, 1e-4), (32, 1e-5))):
     return {"workload": "SU(4) antisymmetric (NF=6), Wilson m0=-0.1, 16^4, U=exp(i0.25H) seed 11, "
                         "phi = D^+ eta; S = phi^+ (H^2)^-1 phi",
             "force_fermion_core_ms": core_ms, "fp64_solve_s": solve_s,
+            "force_fermion_core_ms_by_variant": by_variant,
+            "variants": "1: one thread per link; 2: two threads per link in two warps, projection table in "
+                        "constant memory (default); 3: 2 with L2 prefetches of the link and the spinor at x",
             "algorithmic_bytes": core_bytes + fill_bytes,
             "algorithmic_bytes_note": "X, Y, links and force planes (read + write) of the core, plus the two "
                                       "odd-site fill hops",

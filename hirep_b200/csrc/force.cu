@@ -6,6 +6,8 @@
 // _suNf_FMAT) times the link, projected onto the algebra with the generators of
 // the representation (a sparse table built at lattice set-up), scaled by
 // -residue*dt*C(R)/C(F).  One thread per (site, direction).
+#include <vector>
+
 #include "dirac.cuh"
 
 namespace hrgpu {
@@ -212,6 +214,161 @@ __global__ void __launch_bounds__(128) k_force_hop_w(double *fsum, const void *U
     }
   }
   for (int A = 0; A < P.dimg; A++) fsum[((long)mu * P.dimg + A) * lp + d] += coeff * hs[A * 128 + tid];
+}
+
+// The projection table again, element-major and padded to E entries per
+// element (A = 0, c = 0 for padding), in constant memory: with the element and
+// the entry known at compile time, every coefficient and generator index is a
+// constant operand and the projection needs no loads.  At most 5 entries per
+// element occur (SU(6) fundamental); 3 for the SU(4) two-index antisymmetric,
+// 2 for the SU(3) symmetric and the fundamentals up to SU(3).
+constexpr int FT_MAX = 6 * 6 * 5;
+__constant__ double2 c_ftc[FT_MAX];
+__constant__ int c_ftA[FT_MAX];
+static int ft_E = 0, ft_key = -1;  // entries per element of the uploaded table; (ng, repr) it was made for
+
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+  asm volatile("{\n .reg .u64 g;\n cvta.to.global.u64 g, %0;\n prefetch.global.L2 [g];\n}\n" ::"l"(p));
+}
+
+// k_force_hop_w on two lanes per link, in two different warps: warp w of a
+// block takes pairing h = w & 1 (h = 0: A_k from Y at x+mu, B_k from X at x;
+// h = 1: A_k from X at x+mu, B_k from Y at x) of the sites (w >> 1) * 32 +
+// lane, so a lane holds two U A_k and two B_k instead of four (128 registers,
+// four blocks of 128 per SM against two) and loads half of the spinor
+// components.  The projection is linear, so each lane projects its own terms
+// of every s1 element onto the algebra; the table addresses are then the same
+// for the whole warp and known at compile time (constant operands, no loads
+// and no exchange between lanes), and the two warps' generator sums meet in
+// shared memory at the end, the even generators written by the h = 0 lane and
+// the odd ones by the h = 1 lane.  The four directions of a block of sites are
+// adjacent blocks.  Lanes past the end of the lattice work on site 0 and write
+// nothing, so every lane reaches the barrier.  PF: first ask L2 for the link
+// and the spinor at x (prefetch.global.L2, no registers held), so that their
+// loads, issued a few at a time after the neighbour's, wait for L2 rather than
+// for DRAM.
+template <int N, bool REAL, int E, bool PF>
+__global__ void __launch_bounds__(128, 4) k_force_hop_w3(double *fsum, const void *U, const double2 *X,
+                                                         const double2 *Y, Geo g, int dimg, double coeff) {
+  extern __shared__ double hs[];  // [dimg][128]: this lane's generator sums in column tid
+  const int tid = threadIdx.x, w = tid >> 5, h = w & 1;
+  const long d0 = (long)(blockIdx.x >> 2) * 64 + (w >> 1) * 32 + (tid & 31);
+  const int mu = blockIdx.x & 3;
+  const int p0 = d0 >= g.ld ? 1 : 0;
+  const bool valid = d0 < 2L * g.ld && d0 - p0 * g.ld < g.VH;
+  const long d = valid ? d0 : 0;
+  for (int A = 0; A < dimg; A++) hs[A * 128 + tid] = 0.0;
+  int t, x, y, z;
+  dev_coords(g, (int)d, t, x, y, z);
+  const long dy = nbr_index(g, t, x, y, z, mu, +1);
+  const long lp = 2L * g.ld;
+  const double2 *c2 = h ? X : Y, *c1 = h ? Y : X;
+  if (PF) {
+#pragma unroll
+    for (int e = 0; e < N * N; e++)
+      prefetch_l2(REAL ? (const void *)((const double *)U + ((long)mu * N * N + e) * lp + d)
+                       : (const void *)((const double2 *)U + ((long)mu * N * N + e) * lp + d));
+#pragma unroll
+    for (int c = 0; c < 4 * N; c++) prefetch_l2(sp_at(c1, d, c, g.ld, N));
+  }
+  double2 a[2][N];
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+    const double2 a0 = *sp_at(c2, dy, i, g.ld, N), a1 = *sp_at(c2, dy, N + i, g.ld, N);
+    const double2 a2 = *sp_at(c2, dy, 2 * N + i, g.ld, N), a3 = *sp_at(c2, dy, 3 * N + i, g.ld, N);
+    double2 &pt = a[0][i], &pt2 = a[1][i];
+    if (mu == 0) { pt = cadd(a0, a2); pt2 = cadd(a1, a3); }
+    if (mu == 1) { pt = caddi(a0, a3); pt2 = caddi(a1, a2); }
+    if (mu == 2) { pt = cadd(a0, a3); pt2 = csub(a1, a2); }
+    if (mu == 3) { pt = caddi(a0, a2); pt2 = csubi(a1, a3); }
+  }
+  double2 ua[2][N];
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+    ua[0][i] = ua[1][i] = make_double2(0, 0);
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      const long idx = ((long)mu * N * N + i * N + j) * lp + d;
+      if (REAL) {
+        const double u = ((const double *)U)[idx];
+        rmac(ua[0][i], u, a[0][j]);
+        rmac(ua[1][i], u, a[1][j]);
+      } else {
+        const double2 u = ((const double2 *)U)[idx];
+        cmac(ua[0][i], u, a[0][j]);
+        cmac(ua[1][i], u, a[1][j]);
+      }
+    }
+  }
+  double2 (&b)[2][N] = a;
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+    const double2 b0 = *sp_at(c1, d, i, g.ld, N), b1 = *sp_at(c1, d, N + i, g.ld, N);
+    const double2 b2 = *sp_at(c1, d, 2 * N + i, g.ld, N), b3 = *sp_at(c1, d, 3 * N + i, g.ld, N);
+    double2 &p2 = b[0][i], &p3 = b[1][i];
+    if (mu == 0) { p2 = csub(b0, b2); p3 = csub(b1, b3); }
+    if (mu == 1) { p2 = csubi(b0, b3); p3 = csubi(b1, b2); }
+    if (mu == 2) { p2 = csub(b0, b3); p3 = cadd(b1, b2); }
+    if (mu == 3) { p2 = csubi(b0, b2); p3 = caddi(b1, b3); }
+  }
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      const double mr = ua[0][i].x * b[0][j].x + ua[0][i].y * b[0][j].y + ua[1][i].x * b[1][j].x + ua[1][i].y * b[1][j].y;
+      const double mi =
+          REAL ? 0.0 : ua[0][i].y * b[0][j].x - ua[0][i].x * b[0][j].y + ua[1][i].y * b[1][j].x - ua[1][i].x * b[1][j].y;
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const double2 c = c_ftc[(i * N + j) * E + e];
+        hs[c_ftA[(i * N + j) * E + e] * 128 + tid] += c.x * mr - c.y * mi;
+      }
+    }
+  }
+  __syncthreads();
+  if (valid)
+    for (int A = h; A < dimg; A += 2)
+      fsum[((long)mu * dimg + A) * lp + d] += coeff * (hs[A * 128 + tid] + hs[A * 128 + (tid ^ 32)]);
+}
+
+// the padded table for the current representation, uploaded when it changes
+// (ft_E = 0: some element has more than 5 entries, and k_force_hop_w serves)
+static int force_table_upload() {
+  const int key = L.ng * 16 + L.repr;
+  if (key == ft_key) return 0;
+  const int F2 = L.nf * L.nf, D = L.dimg;
+  auto nz = [&](int A, int k) {
+    return std::hypot(L.h_rT[((size_t)A * F2 + k) * 2], L.h_rT[((size_t)A * F2 + k) * 2 + 1]) > 1e-14;
+  };
+  int emax = 0;
+  for (int k = 0; k < F2; k++) {
+    int n = 0;
+    for (int A = 0; A < D; A++) n += nz(A, k);
+    emax = std::max(emax, n);
+  }
+  const int E = emax <= 2 ? 2 : emax <= 3 ? 3 : 5;
+  ft_E = 0;
+  ft_key = key;
+  if (emax > 5 || F2 * E > FT_MAX) return 0;
+  std::vector<double2> c(FT_MAX, make_double2(0.0, 0.0));
+  std::vector<int> a(FT_MAX, 0);
+  for (int k = 0; k < F2; k++) {
+    int n = 0;
+    for (int A = 0; A < D; A++)
+      if (nz(A, k)) {
+        // c = conj(T_A^R)_k / C(R), as in the table by element
+        const double re = L.h_rT[((size_t)A * F2 + k) * 2], im = L.h_rT[((size_t)A * F2 + k) * 2 + 1];
+        c[k * E + n] = make_double2(re / L.repr_norm2, -im / L.repr_norm2);
+        a[k * E + n] = A;
+        n++;
+      }
+  }
+  ft_key = -1;
+  HR_CUDA(cudaMemcpyToSymbol(c_ftc, c.data(), sizeof(double2) * FT_MAX));
+  HR_CUDA(cudaMemcpyToSymbol(c_ftA, a.data(), sizeof(int) * FT_MAX));
+  ft_E = E;
+  ft_key = key;
+  return 0;
 }
 
 // g5 sigma_{mu nu} on a spinor held as [4][N] (force_fermion_core.c:123-250)
@@ -523,13 +680,38 @@ __global__ void k_force_logdet(double2 *clf, const double *idg, const double2 *i
     }
 }
 
+template <int N, bool REAL, int E>
+static void launch_force_w3(double *fsum, const void *U, const double2 *X, const double2 *Y, Geo g, int dimg,
+                            double coeff, size_t smem, bool pf) {
+  const unsigned grid = 4 * nb(2L * g.ld, 64);
+  if (pf) {
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(k_force_hop_w3<N, REAL, E, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_force_hop_w3<N, REAL, E, true><<<grid, 128, smem, L.stream>>>(fsum, U, X, Y, g, dimg, coeff);
+  } else {
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(k_force_hop_w3<N, REAL, E, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_force_hop_w3<N, REAL, E, false><<<grid, 128, smem, L.stream>>>(fsum, U, X, Y, g, dimg, coeff);
+  }
+}
+
+// variant 1: one lane per link (k_force_hop_w); 2: two lanes per link in two
+// warps with the constant table (k_force_hop_w3); 3: 2 with the L2 prefetches.
+// Variants 2 and 3 need the padded table (ft_E > 0); without it variant 1 runs.
 template <int N, bool REAL>
 static void launch_force_w(double *fsum, const void *U, const double2 *X, const double2 *Y, Geo g, ProjTabK P,
-                           double coeff, size_t smem) {
+                           double coeff, size_t smem, int variant) {
   if constexpr ((!REAL && N <= 6) || (REAL && N == 3)) {
-    if (smem > 48 * 1024)
-      cudaFuncSetAttribute(k_force_hop_w<N, REAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_force_hop_w<N, REAL><<<dim3(nb(2L * g.ld), 4), 128, smem, L.stream>>>(fsum, U, X, Y, g, P, coeff);
+    if (variant >= 2 && ft_E > 0) {
+      const bool pf = variant == 3;
+      if (ft_E == 2) launch_force_w3<N, REAL, 2>(fsum, U, X, Y, g, P.dimg, coeff, smem, pf);
+      else if (ft_E == 3) launch_force_w3<N, REAL, 3>(fsum, U, X, Y, g, P.dimg, coeff, smem, pf);
+      else launch_force_w3<N, REAL, 5>(fsum, U, X, Y, g, P.dimg, coeff, smem, pf);
+    } else {
+      if (smem > 48 * 1024)
+        cudaFuncSetAttribute(k_force_hop_w<N, REAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_force_hop_w<N, REAL><<<dim3(nb(2L * g.ld), 4), 128, smem, L.stream>>>(fsum, U, X, Y, g, P, coeff);
+    }
   }
 }
 
@@ -621,11 +803,19 @@ int hrgpu_force_fermion_core(void *Xs, void *Ys, int auto_fill_odd, double dt, d
     P.c = L.d_projk_c;
     P.dimg = L.dimg;
     const size_t smem = sizeof(double) * 128 * L.dimg;
-    HR_NF_DISPATCH(L.real, L.nf, (launch_force_w<N_, R_>(L.force_sum, L.U, X, Y, g, P, coeff, smem)));
+    if (int rc = force_table_upload()) return rc;
+    const int variant = L.force_variant ? L.force_variant : 2;
+    HR_NF_DISPATCH(L.real, L.nf, (launch_force_w<N_, R_>(L.force_sum, L.U, X, Y, g, P, coeff, smem, variant)));
   } else {
     HR_NF_DISPATCH(L.real, L.nf, (k_force_hop<N_, R_><<<dim3(nb(n), 4), 128, 0, L.stream>>>(L.force_sum, L.U, X, Y, g, proj(), coeff)));
   }
   HR_LAUNCH_CHECK();
+  return 0;
+}
+
+int hrgpu_set_force_variant(int variant) {
+  HR_REQUIRE(variant >= 0 && variant <= 3, HRGPU_E_ARG, "set_force_variant: variant must be 0..3");
+  L.force_variant = variant;
   return 0;
 }
 

@@ -125,6 +125,7 @@ struct Lattice {
   int hopb_force = -1;
   unsigned *hopb_err = nullptr;   // device error word of the tensor-core batch kernel
   int num_sms = 0;                // multiprocessors of the device (persistent grids)
+  int force_variant = 0;          // kernel of the hopping force (0: the measured default)
   // change counters: links (double and float are rewritten together) and the
   // packed clover blocks of each precision; copies made from them record these
   unsigned long gauge_gen = 0, clover_gen[2] = {0, 0};

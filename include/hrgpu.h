@@ -421,6 +421,13 @@ int hrgpu_fermion_force_begin(void);                    /* force_fermion_core.c:
  * by D_oe (times D_oo^-1 with clover) of the even halves, as in the reference. */
 int hrgpu_force_fermion_core(void *Xs, void *Ys, int auto_fill_odd, double dt, double residue);
 int hrgpu_force_clover_logdet(double mass, double residue); /* force_fermion_core.c:777-781; no-op for expclover */
+/* kernel of the hopping part of force_fermion_core for complex NF <= 6 and real
+ * NF = 3: 1 = one thread per link; 2 = two threads per link in two warps (one
+ * per pairing of X and Y) with the algebra projection from a constant-memory
+ * table; 3 = 2 with the link and the spinor at x prefetched into L2; 0 = the
+ * default (2).  A tuning control of this library; it has no counterpart in
+ * the reference. */
+int hrgpu_set_force_variant(int variant);
 /* fermion_force_end (force_fermion_core.c:964-993): clover derivative, then adds the
  * accumulated force to the host momentum field force[V][4][NG*NG-1] (HiRep layout) */
 int hrgpu_fermion_force_end(double dt, double *force_host);

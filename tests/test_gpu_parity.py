@@ -287,6 +287,32 @@ def test_force_matches_oracle(ng, rep, clover):
     assert rel(fg - mom, fo - mom) < 1e-12
 
 
+@pytest.mark.parametrize("variant", [1, 2, 3])
+@pytest.mark.parametrize("ng,rep", [(2, O.FUND), (3, O.FUND), (2, O.ADJ), (4, O.ASYM), (3, O.SYM), (4, O.FUND),
+                                    (5, O.FUND), (6, O.FUND)])
+def test_force_variants(variant, ng, rep):
+    """Every kernel of the hopping force (one lane per link; two lanes per link in two
+    warps with the constant-memory projection table, padded to 2, 3 or 5 entries per
+    element, without and with L2 prefetches) gives the oracle's force, on a
+    4x6x6x6 lattice whose half volume (432) is not a multiple of 32, so the last
+    block holds padding sites that compute and write nothing."""
+    o, lat, _, _ = setup((4, 6, 6, 6), ng, rep, seed=19, smooth=0.3)
+    G._check(lat.L.hrgpu_set_force_variant(variant), "set_force_variant")
+    try:
+        m = -0.1
+        o.set_mass(m)
+        lat.set_dirac_mass(m)
+        X = F.gaussian_spinor(31, o.V, o.nf)
+        Y = F.gaussian_spinor(32, o.V, o.nf)
+        o.fermion_force_begin()
+        o.force_fermion_core(X, Y, 1, 0.7, 1.3)
+        lat.fermion_force_begin()
+        lat.force_fermion_core(lat.field(O.FULL, host=X), lat.field(O.FULL, host=Y), 1, 0.7, 1.3)
+        assert rel(lat.force_sum(), o.force_sum()) < 1e-12
+    finally:
+        G._check(lat.L.hrgpu_set_force_variant(0), "set_force_variant")
+
+
 @pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
 @pytest.mark.parametrize("ng,rep", [(3, O.FUND), (2, O.ADJ), (3, O.SYM)])
 def test_hop_variants(variant, ng, rep):
