@@ -421,6 +421,7 @@ int hrgpu_project_gauge_field(void) {
   const Geo g = make_geo();
   HR_NG_DISPATCH(L.ng, (k_project_suNg<N_><<<dim3(nb128(2L * L.ld), 4), 128, 0, L.stream>>>(L.Ug, g)));
   HR_LAUNCH_CHECK();
+  fund_links_changed();
   return 0;
 }
 
@@ -430,6 +431,7 @@ int hrgpu_update_gauge_field(double dt) {
   const Geo g = make_geo();
   HR_NG_DISPATCH(L.ng, (k_update_gauge<N_><<<dim3(nb128(2L * L.ld), 4), 128, 0, L.stream>>>(L.Ug, L.mom, g_gT, g, L.dimg, dt)));
   HR_LAUNCH_CHECK();
+  fund_links_changed();
   // reunitarise every 17th call, as the reference's counter does (field_update.c:45-57)
   if (g_upd_count & 16) {
     g_upd_count = 0;

@@ -41,7 +41,8 @@ struct HopArgs {
   int g5;
   int nf;
   int cb0, cb1;      // output sites cb0 <= cb < cb1 of parity outp
-  int recon;         // Lattice::recon12 at launch: 2 puts the antiperiodic sign on rebuilt rows
+  int recon;         // Lattice::recon12 at launch: 2 (4) puts the antiperiodic sign on rebuilt rows (links)
+  const double2 *Ug; // fundamental links [4][NG*NG][2ld] (the two-index links built on the fly, recon 3 and 4)
   Geo g;
 };
 
@@ -300,6 +301,75 @@ __device__ __forceinline__ V ld_sel(const V *p, bool smem) {
   return smem ? *p : ld_c(p);
 }
 
+// The two-index representations with NF = 6 built on the fly from the
+// fundamental link u: FR = 1 the symmetric one of SU(3), FR = 2 the
+// antisymmetric one of SU(4).  Element (C, A) of the represented link is the
+// one k_represent writes (the same products and factors, and the boundary
+// sign sg): the columns A and the rows C run over the index pairs (a >= b)
+// and (e <= c) in k_represent's order.  Reading NG^2 instead of 36 complex
+// numbers per link (9 or 16) trades 2.3-4x fewer link bytes for two complex
+// products per element.
+template <int FR>
+struct TwoIdx {
+  static constexpr int NG = FR == 1 ? 3 : 4;
+  // basis element k = 0..5 is the index pair (lo(k), hi(k)): rows C = (e, c) =
+  // (lo, hi), columns A = (a, b) = (hi, lo); symmetric (0,0) (0,1) (1,1) (0,2)
+  // (1,2) (2,2), antisymmetric (0,1) (0,2) (1,2) (0,3) (1,3) (2,3)
+  __host__ __device__ static constexpr int lo(int k) { return (k == 2 || k == 4) ? 1 : (k == 5 ? 2 : 0); }
+  __host__ __device__ static constexpr int hi(int k) { return (k == 0 ? 0 : (k <= 2 ? 1 : 2)) + (FR == 2 ? 1 : 0); }
+};
+
+template <int FR>
+__device__ __forceinline__ double2 two_idx_elem(const double2 (&u)[TwoIdx<FR>::NG * TwoIdx<FR>::NG], int C, int A,
+                                                double sg) {
+  constexpr int N = TwoIdx<FR>::NG;
+  const int e = TwoIdx<FR>::lo(C), c = TwoIdx<FR>::hi(C), a = TwoIdx<FR>::hi(A), b = TwoIdx<FR>::lo(A);
+  auto cm = [](double2 p, double2 q) { return make_double2(p.x * q.x - p.y * q.y, p.x * q.y + p.y * q.x); };
+  if (FR == 1) {
+    // the factors sqrt(2) and 1/sqrt(2) as constants (k_represent divides by
+    // sqrt(2): the elements may differ from the stored ones in the last bit)
+    constexpr double st = 1.4142135623730951, ist = 0.7071067811865476;
+    const bool diag = a == b;
+    const double2 mf = diag ? cm(u[e * N + a], u[c * N + a]) : cadd(cm(u[e * N + a], u[c * N + b]), cm(u[e * N + b], u[c * N + a]));
+    double2 w;
+    if (e < c) w = diag ? make_double2(mf.x * st, mf.y * st) : mf;
+    else w = diag ? mf : make_double2(mf.x * ist, mf.y * ist);
+    return make_double2(sg * w.x, sg * w.y);
+  } else {
+    const double2 mf = csub(cm(u[e * N + a], u[c * N + b]), cm(u[e * N + b], u[c * N + a]));
+    return make_double2(-sg * mf.x, -sg * mf.y);
+  }
+}
+
+// c0 = U^R h0, c1 = U^R h1 (DAG: U^R+) with U^R built from the fundamental link
+// at `site` of the planes Ug (plane stride `plane`)
+template <int FR, bool DAG>
+__device__ __forceinline__ void two_idx_mul2(double2 *c0, double2 *c1, const double2 *h0, const double2 *h1,
+                                             const double2 *Ug, long plane, long site, double sg) {
+  constexpr int N = TwoIdx<FR>::NG;
+  double2 u[N * N];
+#pragma unroll
+  for (int k = 0; k < N * N; k++) u[k] = ld_c(Ug + (long)k * plane + site);
+#pragma unroll
+  for (int i = 0; i < 6; i++) {
+    double2 a0 = make_double2(0.0, 0.0), a1 = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+      if (!DAG) {
+        const double2 v = two_idx_elem<FR>(u, i, j, sg);
+        cmac(a0, v, h0[j]);
+        cmac(a1, v, h1[j]);
+      } else {
+        const double2 v = two_idx_elem<FR>(u, j, i, sg);
+        cmacc(a0, v, h0[j]);
+        cmacc(a1, v, h1[j]);
+      }
+    }
+    c0[i] = a0;
+    c1[i] = a1;
+  }
+}
+
 // one output site (checkerboard index cb < VH) of the hop; returns |out|^2 when a.red is set
 // LE: the storage type of a link element (BF16 for the FP32 operator's optional link copy)
 // TSM: the t+1 / t-1 neighbours come from shared memory (tsu, tsd: this thread's
@@ -307,7 +377,7 @@ __device__ __forceinline__ V ld_sel(const V *p, bool smem) {
 // the mbarrier at shared address bar have landed; the t direction is then
 // visited last, after x, y, z, to give the copies time
 template <int NFT, bool REAL, typename R, int EP, typename LE = typename LinkE<REAL, R>::T, bool TSM = false,
-          bool RC = false>
+          bool RC = false, int FR = 0>
 __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb, const typename C2<R>::T *tsu = nullptr,
                                            const typename C2<R>::T *tsd = nullptr, unsigned bar = 0) {
   typedef typename C2<R>::T V;
@@ -356,8 +426,14 @@ __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb, co
           if (mu == 2) { h0[i] = cadd(s0, s3); h1[i] = csub(s1, s2); }
           if (mu == 3) { h0[i] = caddi(s0, s2); h1[i] = csubi(s1, s3); }
         }
-        const R sgf = (a.recon == 2 && mu == 0 && t == 0) ? (R)-1 : (R)1;
-        link_mul2<NA, false, R12, R12R>(c0, c1, h0, h1, Umu, lplane, so, nf, sgf);
+        if constexpr (FR != 0) {
+          const double sgr = (a.recon == 4 && mu == 0 && t == 0) ? -1.0 : 1.0;
+          two_idx_mul2<FR, false>(c0, c1, h0, h1, a.Ug + (long)mu * TwoIdx<FR>::NG * TwoIdx<FR>::NG * lplane, lplane,
+                                  so, sgr);
+        } else {
+          const R sgf = (a.recon == 2 && mu == 0 && t == 0) ? (R)-1 : (R)1;
+          link_mul2<NA, false, R12, R12R>(c0, c1, h0, h1, Umu, lplane, so, nf, sgf);
+        }
 #pragma unroll
         for (int i = 0; i < NA; i++) {
           if (i >= nf) break;
@@ -384,8 +460,14 @@ __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb, co
           if (mu == 3) { h0[i] = csubi(s0, s2); h1[i] = caddi(s1, s3); }
         }
         const long sn = (long)inp * g.ld + cdn;
-        const R sgb = (a.recon == 2 && mu == 0 && tm == 0) ? (R)-1 : (R)1;
-        link_mul2<NA, true, R12, R12R>(c0, c1, h0, h1, Umu, lplane, sn, nf, sgb);
+        if constexpr (FR != 0) {
+          const double sgr = (a.recon == 4 && mu == 0 && tm == 0) ? -1.0 : 1.0;
+          two_idx_mul2<FR, true>(c0, c1, h0, h1, a.Ug + (long)mu * TwoIdx<FR>::NG * TwoIdx<FR>::NG * lplane, lplane,
+                                 sn, sgr);
+        } else {
+          const R sgb = (a.recon == 2 && mu == 0 && tm == 0) ? (R)-1 : (R)1;
+          link_mul2<NA, true, R12, R12R>(c0, c1, h0, h1, Umu, lplane, sn, nf, sgb);
+        }
 #pragma unroll
         for (int i = 0; i < NA; i++) {
           if (i >= nf) break;
@@ -454,14 +536,16 @@ __device__ __forceinline__ void pdl_enter() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
-// RC: rebuild row 2 of the 3x3 links (instantiated for NF = 3 only)
-template <int NFT, bool REAL, typename R, int EP, int MINB, typename LE = typename LinkE<REAL, R>::T, bool RC = false>
+// RC: rebuild row 2 of the 3x3 links (instantiated for NF = 3 only); FR: build
+// the NF = 6 two-index links from the fundamental ones (FP64, see TwoIdx)
+template <int NFT, bool REAL, typename R, int EP, int MINB, typename LE = typename LinkE<REAL, R>::T, bool RC = false,
+          int FR = 0>
 __global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop(HopArgs<R> a) {
   pdl_enter();
   if (a.stop && *a.stop) return;
   const int cb = a.cb0 + blockIdx.x * blockDim.x + threadIdx.x;
   double nrm = 0.0;
-  if (cb < a.cb1) nrm = hop_site<NFT, REAL, R, EP, LE, false, RC>(a, cb);
+  if (cb < a.cb1) nrm = hop_site<NFT, REAL, R, EP, LE, false, RC, FR>(a, cb);
   if (a.red) block_partial<R>(nrm, a.red);
 }
 

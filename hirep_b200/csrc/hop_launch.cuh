@@ -79,6 +79,23 @@ static inline void (*hop_kernel(int recon))(HopArgs<R>) {
   return k_hop<N, RL, R, EP, MINB>;
 }
 
+// variant 6: k_hop (variant 0's register budget) building the NF = 6
+// two-index links from the fundamental ones, FP64, while the fundamental links
+// are those the represented field was made from (link modes 3 and 4); -1 otherwise
+template <int N, bool RL, typename R, int EP>
+int launch_fund(HopArgs<R> &a, dim3 grid, dim3 block, cudaStream_t s) {
+  if constexpr (N == 6 && !RL && sizeof(R) == 8) {
+    if (a.recon < 3) return -1;
+    if (L.repr == HRGPU_SYM)
+      HR_CUDA(launch_pdl<R>(k_hop<N, RL, R, EP, 1, typename LinkE<RL, R>::T, false, 1>, grid, block, 0, s, a));
+    else
+      HR_CUDA(launch_pdl<R>(k_hop<N, RL, R, EP, 1, typename LinkE<RL, R>::T, false, 2>, grid, block, 0, s, a));
+    return 0;
+  } else {
+    return -1;
+  }
+}
+
 template <typename R, int EP>
 int launch_ep_variant(HopArgs<R> &a, int variant) {
   a.g = make_geo();
@@ -87,7 +104,8 @@ int launch_ep_variant(HopArgs<R> &a, int variant) {
   // variants: 0 one thread per site, 1 two threads per site (spin split),
   // 2 and 3 the same with the register budget capped for 4 resident blocks per SM,
   // 4 one thread per site with the per-direction loads pipelined through shared memory,
-  // 5 one thread per site with the time halo staged by bulk (TMA) copies
+  // 5 one thread per site with the time halo staged by bulk (TMA) copies,
+  // 6 one thread per site building the NF = 6 two-index links from the fundamental ones
   const long nsites = a.cb1 - a.cb0;
   const long threads = hop_threads_per_site(variant) * nsites;
   dim3 grid((unsigned)((threads + HOP_THREADS - 1) / HOP_THREADS)), block(HOP_THREADS);
@@ -102,8 +120,11 @@ int launch_ep_variant(HopArgs<R> &a, int variant) {
       case 4:                                                                          \
         if (int rc_ = launch_async<N, RL, R, EP>(a, grid, block, s)) return rc_;       \
         break;                                                                         \
-      default:                                                                         \
+      case 5:                                                                          \
         if (int rc_ = launch_tma<N, RL, R, EP>(a, grid, block, s)) return rc_;         \
+        break;                                                                         \
+      default:                                                                         \
+        if (int rc_ = launch_fund<N, RL, R, EP>(a, grid, block, s)) return rc_;        \
         break;                                                                         \
     }                                                                                  \
     break;

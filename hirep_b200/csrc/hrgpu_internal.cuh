@@ -48,7 +48,7 @@ int fail_cuda(cudaError_t e, const char *what, const char *file, int line);
 constexpr int MAXNF = 64;
 constexpr int RED_THREADS = 256;
 constexpr int RED_MAX_BLOCKS = 1184;  // 8 x 148 SMs
-constexpr int HOP_VARIANTS = 6;
+constexpr int HOP_VARIANTS = 7;
 constexpr int HOPB_VARIANTS = 5;   // batch hopping kernel variants (3, 4: tensor cores)
 constexpr int HOPB_MAXNB = 64;     // fields per batch
 
@@ -148,6 +148,7 @@ int ensure_tmp(void **p, size_t bytes);
 int library_device();  // the device of hrgpu_init (-1 before)
 int ensure_links_bf16();  // the BF16 copy of the links, made from the FP64 ones when they changed
 int detect_recon12();     // check links set already represented for row-2 reconstruction
+void fund_links_changed(); // the fundamental links were written: stop building represented links from them
 int compute_clover_term_dev();
 void cg_release();
 int ensure_stage(size_t bytes);

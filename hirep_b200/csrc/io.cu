@@ -202,6 +202,7 @@ int hrgpu_read_gauge_field(const char *filename, double *plaq_file, double *plaq
   if (e == cudaSuccess) {
     k_file_to_links<<<io_grid(4L * L.V), 256, 0, L.stream>>>(L.Ug, dbuf, g, n2, quat);
     e = cudaGetLastError();
+    fund_links_changed();
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(L.stream);
   cudaFree(dbuf);

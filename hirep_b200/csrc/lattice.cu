@@ -647,6 +647,7 @@ int hrgpu_gauge_set(const double *u_host) {
   long n = L.V * 4 * nel;
   k_links_in<double2><<<nblk(n), 256, 0, L.stream>>>(L.Ug, (const double2 *)L.stage, L.d_h2d, L.V, nel, L.ld);
   HR_LAUNCH_CHECK();
+  fund_links_changed();
   HR_CUDA(cudaStreamSynchronize(L.stream));
   L.have_fund = true;
   return 0;

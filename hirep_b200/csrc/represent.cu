@@ -166,8 +166,19 @@ __global__ void k_check_row2_real(const double *U, Geo g, int bc, double tol, in
 // The hopping kernels may rebuild row 2 of the SU(3) fundamental or SU(2)
 // adjoint links when every link passes the check at 1e-14 (unitary links of
 // determinant 1, up to the boundary sign); otherwise they read the full links.
-static int set_recon12(int bc) {
+// For the NF = 6 two-index representations (SU(3) symmetric, SU(4)
+// antisymmetric) the FP64 kernels may build the links from the fundamental ones
+// (modes 3, and 4 with the antiperiodic sign) as long as the fundamental field
+// is the one the represented field was made from: set by
+// represent_gauge_field, cleared by whatever writes the fundamental links
+// (fund_links_changed) or uploads represented links.
+static int set_recon12(int bc, bool from_fund) {
   L.recon12 = 0;
+  const bool two6 = !L.real && L.nf == 6 && ((L.repr == HRGPU_SYM && L.ng == 3) || (L.repr == HRGPU_ASYM && L.ng == 4));
+  if (two6) {
+    if (from_fund && L.Ug) L.recon12 = bc ? 4 : 3;
+    return 0;
+  }
   const bool su3 = !L.real && L.nf == 3 && L.ng == 3 && L.repr == HRGPU_FUND;
   const bool so3 = L.real && L.nf == 3 && L.ng == 2 && L.repr == HRGPU_ADJ;
   if (!su3 && !so3) return 0;
@@ -191,10 +202,14 @@ static int set_recon12(int bc) {
 // links uploaded already represented (hrgpu_gauge_set_f): the boundary
 // condition is not known, so try the antiperiodic sign, then none
 int detect_recon12() {
-  if (int rc = set_recon12(1)) return rc;
+  if (int rc = set_recon12(1, false)) return rc;
   if (L.recon12 == 0)
-    if (int rc = set_recon12(0)) return rc;
+    if (int rc = set_recon12(0, false)) return rc;
   return 0;
+}
+
+void fund_links_changed() {
+  if (L.recon12 >= 3) L.recon12 = 0;
 }
 
 }  // namespace hrgpu
@@ -226,7 +241,7 @@ int hrgpu_represent_gauge_field(int bc_t_antiperiodic) {
   HR_LAUNCH_CHECK();
   L.have_gauge = true;
   L.bc_t = bc_t_antiperiodic;
-  if (int rc = set_recon12(bc_t_antiperiodic)) return rc;
+  if (int rc = set_recon12(bc_t_antiperiodic, true)) return rc;
   if (int rc = hrgpu_assign_ud2u_f()) return rc;
   if (L.clover) {
     if (int rc = compute_clover_term_dev()) return rc;

@@ -99,11 +99,19 @@ int hrgpu_represent_gauge_field(int bc_t_antiperiodic);
  * to 1e-14 (s = -1 on the links with the antiperiodic time sign), the
  * single-field hopping kernels load rows 0 and 1 only and rebuild row 2.
  * hrgpu_gauge_set_f runs the same check, trying the antiperiodic sign first.
+ * The SU(3) symmetric and SU(4) antisymmetric representations (NF = 6): after
+ * represent_gauge_field the FP64 single-field hopping kernel of variant 6 may
+ * build each represented link from the fundamental one (9 or 16 complex
+ * numbers read instead of 36), until the fundamental links are written again
+ * (hrgpu_gauge_set, update_gauge_field, project_gauge_field,
+ * read_gauge_field) or represented links are uploaded; the autotuner times it
+ * against the other variants.
  * mode: 0 full links (any other group or representation, a field that fails
- * the check), 1 rebuilt, 2 rebuilt with the antiperiodic sign.  No counterpart
- * in the reference, which reads the full links. */
+ * the check), 1 rebuilt, 2 rebuilt with the antiperiodic sign, 3 built from
+ * the fundamental links, 4 the same with the antiperiodic sign.  No
+ * counterpart in the reference, which reads the full links. */
 int hrgpu_link_recon(int *mode);
-/* allow (1, default) or forbid (0) the row-2 reconstruction above */
+/* allow (1, default) or forbid (0) the reconstruction modes above */
 int hrgpu_set_link_recon(int on);
 /* u_gauge_f upload: the represented field as HiRep holds it ([V][4][NF*NF], complex,
  * or real for the adjoint representation) */
@@ -154,10 +162,13 @@ int hrgpu_g5Dphi_eopre_sq_flt(double m0, void *out, const void *in);
  * 4 = one thread per site with cp.async-pipelined loads, 5 = one thread per site
  * with the time halo staged in shared memory by bulk (TMA) copies (4 and 5: NF <= 4
  * complex, NF = 3 real; 5 also needs time slabs of a multiple of 128 sites per
- * parity), -1 = autotune on first use (default).  hrgpu_hop_tuning reports the
- * variant chosen for (precision, epilogue 0..2) and the per-launch times it
- * measured (ms has room for 6 values; -1 marks a variant not built for this
- * NF or lattice); precision 2 is the FP32 operator reading BF16 links.
+ * parity), 6 = one thread per site building the SU(3) symmetric or SU(4)
+ * antisymmetric links from the fundamental ones (FP64, link modes 3 and 4 of
+ * hrgpu_link_recon), -1 = autotune on first use (default).  hrgpu_hop_tuning
+ * reports the variant chosen for (precision, epilogue 0..2) and the per-launch
+ * times it measured (ms has room for 7 values; -1 marks a variant not built for
+ * this NF, lattice or link mode); precision 2 is the FP32 operator reading BF16
+ * links.
  * Tuning controls of this library; they have no counterpart in the reference. */
 int hrgpu_set_hop_variant(int variant);
 int hrgpu_hop_tuning(int prec, int epilogue, int *chosen, float *ms);

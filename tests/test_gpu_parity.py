@@ -313,7 +313,7 @@ def test_force_variants(variant, ng, rep):
         G._check(lat.L.hrgpu_set_force_variant(0), "set_force_variant")
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("ng,rep", [(3, O.FUND), (2, O.ADJ), (3, O.SYM)])
 def test_hop_variants(variant, ng, rep):
     """Every variant of the hopping kernel the autotuner can pick gives the oracle's
