@@ -246,6 +246,9 @@ def main():
     ap.add_argument("--hmc-only", action="store_true", help="only the HMC trajectories (32^3x64 SU(2) adjoint)")
     ap.add_argument("--force-only", action="store_true",
                     help="only the force leg, without finite differences (for profiling its kernels)")
+    ap.add_argument("--dslash-config", type=int, default=None, metavar="K",
+                    help="only the single-field operator leg of workload K of the other configurations "
+                         "(0: 16^4 SU(4) antisymmetric, 1: 24^3x48 sextet clover, 2: 32^3x64 SU(2) adjoint)")
     ap.add_argument("--batch-op", default=None, metavar="TxXxYxZ",
                     help="only time the batched g5Cphi_eopre of the batched workload on this lattice")
     ap.add_argument("--nb", type=int, default=12, help="fields per batch for --batch-op")
@@ -270,6 +273,13 @@ def main():
     torch.cuda.set_device(local)
     if args.batch_op:
         return batch_op_main(args, torch, G, F)
+    if args.dslash_config is not None:
+        stream = torch.cuda.current_stream()
+        flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+        peak, _ = measured_peak()
+        out = run_dslash_configs(torch, stream, G, F, flush.zero_, peak, only=args.dslash_config)
+        print(json.dumps({"dslash_configs": out}), flush=True)
+        return
     if args.force_only:
         print(json.dumps({"force": run_force_check(torch, torch.cuda.current_stream(), G, F, fd=())}), flush=True)
         return
@@ -434,12 +444,14 @@ DSLASH_CONFIGS = [
 ]
 
 
-def run_dslash_configs(torch, stream, G, F, flush_l2, peak, steps=50):
+def run_dslash_configs(torch, stream, G, F, flush_l2, peak, steps=50, only=None):
     """FP64 even-odd operator per workload: device time per application (L2
     flushed between steps, CUDA events), HiRep-model GB/s and the fraction of
     the measured HBM peak on the bytes it must move at least."""
     out = []
-    for name, dims, ng, rep, csw, m, eps, seed in DSLASH_CONFIGS:
+    for k, (name, dims, ng, rep, csw, m, eps, seed) in enumerate(DSLASH_CONFIGS):
+        if only is not None and k != only:
+            continue
         lat = G.Lattice(*dims, ng, getattr(G, rep))
         lat.set_gauge(F.smooth_gauge(seed, lat.V, ng, eps))
         lat.represent_gauge_field(True)
