@@ -291,6 +291,9 @@ int launch_ep(HopArgs<R> &a) {
     v = bestv;
   }
   int rc = launch_ep_variant<R, EP>(a, v);
+  // variant 6 chosen while the links could be built from the fundamental ones,
+  // and the fundamental links written since: the stored links, variant 0
+  if (rc < 0 && v == 6) rc = launch_ep_variant<R, EP>(a, 0);
   if (rc < 0) {
     set_error("hopping-kernel variant %d is not built for NF=%d", v, L.nf);
     return HRGPU_E_NF;

@@ -102,6 +102,22 @@ def test_fundamental_write_ends_the_mode(ng, rep):
         G._check(lat.L.hrgpu_set_hop_variant(-1), "set_hop_variant")
 
 
+def test_tuned_variant_survives_the_end_of_the_mode():
+    """The autotuner picks variant 6; after new fundamental links without
+    represent_gauge_field the operator runs on the stored links (variant 0)."""
+    o, u, lat = make(4, O.ASYM, True, dims=(4, 8, 8, 8))
+    m = -0.2
+    e = F.gaussian_spinor(9, o.VH, o.nf)
+    fe, out = lat.field(O.EVEN, host=e), lat.field(O.EVEN)
+    lat.Dphi_eopre(m, out, fe)  # tunes the FP64 hops
+    ref = o.Dphi_eopre(m, e)
+    assert rel(out.download(), ref) < TOL64
+    lat.set_gauge(F.smooth_gauge(98, o.V, 4, 0.3))  # hrgpu_gauge_set only: the mode ends
+    assert lat.link_recon() == 0
+    lat.Dphi_eopre(m, out, fe)
+    assert rel(out.download(), ref) < TOL64
+
+
 def test_uploaded_represented_links_use_the_stored_form():
     """Links uploaded already represented (hrgpu_gauge_set_f) give mode 0."""
     o = O.Oracle(4, 4, 4, 4, 3, O.SYM)
