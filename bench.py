@@ -486,7 +486,19 @@ def run_dslash_configs(torch, stream, G, F, flush_l2, peak, steps=50, only=None)
         fund = mode >= 3 and all(tun.get(k, {}).get("variant") == 6 for k in used)
         rows = 2 if mode in (1, 2) else nf
         ub = unique_bytes(lat.V, nf, real, rows, csw is not None, link_bytes=ng * ng * 16 if fund else None)
-        out.append({"workload": name, "ms_per_application": ms, "hirep_model_GBps": model / (ms * 1e-3) / 1e9,
+        extra = {}
+        if csw is not None:
+            # compute_clover_term (the clover term from the links; once per gauge field)
+            ev = []
+            for _ in range(5):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                lat.compute_clover_term()
+                b.record(stream)
+                ev.append((a, b))
+            torch.cuda.synchronize()
+            extra["compute_clover_term_ms"] = float(np.median([a.elapsed_time(b) for a, b in ev]))
+        out.append({"workload": name, "ms_per_application": ms, "hirep_model_GBps": model / (ms * 1e-3) / 1e9, **extra,
                     "algorithmic_bytes": ub, "achieved_GBps": ub / (ms * 1e-3) / 1e9,
                     "frac_of_measured_hbm": ub / (ms * 1e-3) / 1e9 / peak,
                     "links_read": "fundamental" if fund else f"{rows} of {nf} rows",

@@ -100,6 +100,21 @@ def test_float_operators(ng, rep):
     assert rel(out_e.download(), d) < 1e-5
 
 
+@pytest.mark.parametrize("dims", [(4, 4, 4, 4), (4, 6, 6, 6)])
+@pytest.mark.parametrize("ng,rep", [(2, O.FUND), (3, O.FUND), (4, O.FUND), (2, O.ADJ), (3, O.ADJ), (4, O.ADJ),
+                                    (3, O.SYM), (4, O.SYM), (4, O.ASYM), (5, O.ASYM)])
+def test_clover_term_every_representation(dims, ng, rep):
+    """compute_clover_term (one thread per site, plane and row; several sites per
+    block) against the oracle element by element for every NF the library builds,
+    complex and real, on a lattice whose last block is ragged (4^4) and one with
+    padding sites (half volume 432)."""
+    o, lat, _, _ = setup(dims, ng, rep, seed=5, smooth=0.3)
+    o.clover_init(1.0)
+    o.compute_clover_term()
+    lat.clover_init(1.0)
+    assert rel(lat.clover_term(), o.clover_term()) < TOL64
+
+
 @pytest.mark.parametrize("ng,rep", [(3, O.FUND), (2, O.ADJ), (3, O.SYM), (2, O.FUND)])
 def test_clover_operators(ng, rep):
     o, lat, _, _ = setup((4, 4, 4, 4), ng, rep, seed=5, smooth=0.3)
