@@ -364,21 +364,22 @@ def main():
         lat.Cphi_eopre(MASS, fout, fin)
         G._check(lat.L.hrgpu_spinor_download(p_out, fout.ptr, G.EVEN, G.DOUBLE), "download")
 
-    def time_e2e(fn):
+    def time_e2e(fn, extra_warmup=0):
         ts = []
-        for k in range(args.warmup + min(args.steps, 200)):
+        warm = args.warmup + extra_warmup
+        for k in range(warm + min(args.steps, 200)):
             flush_l2()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
             fn()
             b.record(stream)
             torch.cuda.synchronize()
-            if k >= args.warmup:
+            if k >= warm:
                 ts.append(a.elapsed_time(b))
         return max_over_ranks(float(np.mean(ts)), dist, "cuda")
 
     lat.set_host_chunks(args.host_chunks)
-    e2e_ms = time_e2e(e2e_pipelined)
+    e2e_ms = time_e2e(e2e_pipelined, extra_warmup=8)  # the first 8 calls choose the form
     e2e_seq_ms = time_e2e(e2e_sequential)
     form, ms_pipe, ms_seq = G.ctypes.c_int(), G.ctypes.c_float(), G.ctypes.c_float()
     G._check(lat.L.hrgpu_host_form(G.ctypes.byref(form), G.ctypes.byref(ms_pipe), G.ctypes.byref(ms_seq)),

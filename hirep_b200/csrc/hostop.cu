@@ -41,8 +41,10 @@
 // smaller copies of the pipeline lose to one copy each way.  So when a graph
 // is made for a new key, the plain sequence (one copy in, the operator on the
 // whole lattice, one copy out) is captured beside it, both are replayed and
-// timed on the spot, and the faster is kept for that key
+// timed on the spot, and the first calls for that key then alternate the two
+// and keep the one with the lower mean device time per call
 // (hrgpu_set_host_form pins one form, hrgpu_host_form reports the choice).
+#include <utility>
 #include <vector>
 
 #include "dirac.cuh"
@@ -77,13 +79,21 @@ struct HostGraph {
   int v0, v1, flt_links, pdl;
   long VH;
   cudaGraphExec_t exec = nullptr;
+  // form 0 (auto): the other form's graph while the first calls try both
+  cudaGraphExec_t alt = nullptr;
+  int trials = 0;
+  double tsum[2] = {0.0, 0.0};  // GPU time of the trial calls, by form (pipelined, sequential)
+  int tn[2] = {0, 0};
 };
+constexpr int HP_TRIALS = 8;  // calls that alternate the two forms before one is kept
 static std::vector<HostGraph> HG;  // a few cached graphs
 constexpr size_t HG_MAX = 8;
 
 static void free_graphs() {
-  for (HostGraph &h : HG)
+  for (HostGraph &h : HG) {
     if (h.exec) cudaGraphExecDestroy(h.exec);
+    if (h.alt) cudaGraphExecDestroy(h.alt);
+  }
   HG.clear();
 }
 
@@ -387,8 +397,8 @@ static int apply_host(int clover, int g5, double mass, void *host_out, const voi
         return rc;
       }
       const int keep = !ex[0] ? 1 : !ex[1] ? 0 : (ms[1] < ms[0] ? 1 : 0);
-      if (ex[1 - keep]) cudaGraphExecDestroy(ex[1 - keep]);
       key.exec = ex[keep];
+      key.alt = ex[1 - keep];  // kept for the trial calls when both forms exist
       key.form = keep ? FORM_SEQUENTIAL : FORM_PIPELINED;
       hp_last_form = key.form;
       hp_last_ms[0] = ms[0];
@@ -396,7 +406,41 @@ static int apply_host(int clover, int g5, double mass, void *host_out, const voi
       HG.push_back(key);
       hit = &HG.back();
     }
-    HR_CUDA(cudaGraphLaunch(hit->exec, L.stream));
+    if (!hit->alt) {
+      HR_CUDA(cudaGraphLaunch(hit->exec, L.stream));
+    } else {
+      // The replays timed when the graphs were made run back to back; the calls
+      // of a program come with host work between them, and on some hosts the
+      // order of the two forms differs between the two patterns.  So the first
+      // HP_TRIALS calls alternate the forms, timed on the device, and the form
+      // with the lower mean is kept (the results are bit-identical).
+      static cudaEvent_t te[2] = {nullptr, nullptr};
+      if (!te[0]) {
+        HR_CUDA(cudaEventCreate(&te[0]));
+        HR_CUDA(cudaEventCreate(&te[1]));
+      }
+      const bool use_alt = hit->trials & 1;
+      const int f = (hit->form == FORM_PIPELINED) != use_alt ? 0 : 1;  // 0 pipelined, 1 sequential
+      HR_CUDA(cudaEventRecord(te[0], L.stream));
+      HR_CUDA(cudaGraphLaunch(use_alt ? hit->alt : hit->exec, L.stream));
+      HR_CUDA(cudaEventRecord(te[1], L.stream));
+      HR_CUDA(cudaStreamSynchronize(L.stream));
+      float ms = 0;
+      HR_CUDA(cudaEventElapsedTime(&ms, te[0], te[1]));
+      hit->tsum[f] += ms;
+      hit->tn[f]++;
+      if (++hit->trials >= HP_TRIALS) {
+        const double m0 = hit->tsum[0] / hit->tn[0], m1 = hit->tsum[1] / hit->tn[1];
+        const int best = m1 < m0 ? FORM_SEQUENTIAL : FORM_PIPELINED;
+        if (best != hit->form) std::swap(hit->exec, hit->alt);
+        cudaGraphExecDestroy(hit->alt);
+        hit->alt = nullptr;
+        hit->form = best;
+        hp_last_form = best;
+        hp_last_ms[0] = (float)m0;
+        hp_last_ms[1] = (float)m1;
+      }
+    }
   }
   HR_CUDA(cudaStreamSynchronize(L.stream));
   add_mvm(2);  // the two hops of one application, as the whole-lattice operator counts them

@@ -211,11 +211,14 @@ int hrgpu_set_host_chunks(int chunks); /* chunks of the pipeline (default 10; 1 
 /* With pinned buffers the operator runs as a cached CUDA graph per (operator,
  * mass, buffers, ...).  Form 0 (default): when a graph is made, the pipelined
  * form and the plain sequence (one copy each way around the whole-lattice
- * operator) are both captured and timed, and the faster is kept; 1 forces the
- * pipeline, 2 the plain sequence.  No HiRep counterpart (host-field transport). */
+ * operator) are both captured and timed, the faster is used first, the first 8
+ * calls for that graph alternate the two (timed on the device) and the one with
+ * the lower mean is kept; 1 forces the pipeline, 2 the plain sequence.  No
+ * HiRep counterpart (host-field transport). */
 int hrgpu_set_host_form(int form);
 /* the form chosen for the last graph made (1 pipelined, 2 sequential, -1 none
- * yet) and the replay times measured for that choice (ms; -1 if not timed) */
+ * yet) and the times behind the choice (ms: the replays when the graph was made,
+ * then the trial calls' means once they are done; -1 if not timed) */
 int hrgpu_host_form(int *form, float *ms_pipelined, float *ms_sequential);
 
 /* ---------------------------------------------------------------- clover -- */
