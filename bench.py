@@ -488,6 +488,25 @@ def run_dslash_configs(torch, stream, G, F, flush_l2, peak, steps=50, only=None)
         rows = 2 if mode in (1, 2) else nf
         ub = unique_bytes(lat.V, nf, real, rows, csw is not None, link_bytes=ng * ng * 16 if fund else None)
         extra = {}
+        # the FP32 operator (the inner solves of the mixed-precision CG), same workload
+        f32in = lat.field(G.EVEN, G.FLOAT, host=F.gaussian_spinor(seed, lat.VH, nf).astype(np.complex64))
+        f32out = lat.field(G.EVEN, G.FLOAT)
+        op32 = lat.g5Cphi_eopre_flt if csw is not None else lat.Dphi_eopre_flt
+        for _ in range(5):
+            op32(m, f32out, f32in)
+        torch.cuda.synchronize()
+        ts32 = []
+        for _ in range(steps):
+            flush_l2()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            op32(m, f32out, f32in)
+            b.record(stream)
+            ts32.append((a, b))
+        torch.cuda.synchronize()
+        extra["fp32_ms_per_application"] = float(np.mean([a.elapsed_time(b) for a, b in ts32]))
+        t32 = hop_tuning(lat, G)
+        extra["fp32_hop_tuning"] = {k: t32.get(k) for k in ("f32_axpy", "f32_clover_inv", "f32_clover") if k in t32}
         if csw is not None:
             # compute_clover_term (the clover term from the links; once per gauge field)
             ev = []

@@ -46,7 +46,7 @@ int hop(int outp, void *out, const void *in, int ep, double cacc, const void *au
   a.g5 = g5;
   a.stop = L.cur_stop;
   a.err = nullptr;
-  a.Ug = L.Ug;
+  a.Ug = sizeof(R) == 8 ? (const void *)L.Ug : (const void *)L.Ugf;
   if (sizeof(R) == 4 && L.flt_links == HRGPU_LINKS_BF16) {
     if (int rc = ensure_links_bf16()) return rc;
     a.U = L.Ubf;

@@ -42,7 +42,7 @@ struct HopArgs {
   int nf;
   int cb0, cb1;      // output sites cb0 <= cb < cb1 of parity outp
   int recon;         // Lattice::recon12 at launch: 2 (4) puts the antiperiodic sign on rebuilt rows (links)
-  const double2 *Ug; // fundamental links [4][NG*NG][2ld] (the two-index links built on the fly, recon 3 and 4)
+  const void *Ug;    // fundamental links [4][NG*NG][2ld], element type of R (two-index links built on the fly, recon 3, 4)
   Geo g;
 };
 
@@ -319,48 +319,55 @@ struct TwoIdx {
   __host__ __device__ static constexpr int hi(int k) { return (k == 0 ? 0 : (k <= 2 ? 1 : 2)) + (FR == 2 ? 1 : 0); }
 };
 
-template <int FR>
-__device__ __forceinline__ double2 two_idx_elem(const double2 (&u)[TwoIdx<FR>::NG * TwoIdx<FR>::NG], int C, int A,
-                                                double sg) {
+template <int FR, typename V>
+__device__ __forceinline__ V two_idx_elem(const V (&u)[TwoIdx<FR>::NG * TwoIdx<FR>::NG], int C, int A,
+                                          decltype(V::x) sg) {
+  typedef decltype(V::x) R;
   constexpr int N = TwoIdx<FR>::NG;
   const int e = TwoIdx<FR>::lo(C), c = TwoIdx<FR>::hi(C), a = TwoIdx<FR>::hi(A), b = TwoIdx<FR>::lo(A);
-  auto cm = [](double2 p, double2 q) { return make_double2(p.x * q.x - p.y * q.y, p.x * q.y + p.y * q.x); };
+  auto mk = [](R x, R y) {
+    V r;
+    r.x = x;
+    r.y = y;
+    return r;
+  };
+  auto cm = [&](V p, V q) { return mk(p.x * q.x - p.y * q.y, p.x * q.y + p.y * q.x); };
   if (FR == 1) {
     // the factors sqrt(2) and 1/sqrt(2) as constants (k_represent divides by
     // sqrt(2): the elements may differ from the stored ones in the last bit)
-    constexpr double st = 1.4142135623730951, ist = 0.7071067811865476;
+    constexpr R st = (R)1.4142135623730951, ist = (R)0.7071067811865476;
     const bool diag = a == b;
-    const double2 mf = diag ? cm(u[e * N + a], u[c * N + a]) : cadd(cm(u[e * N + a], u[c * N + b]), cm(u[e * N + b], u[c * N + a]));
-    double2 w;
-    if (e < c) w = diag ? make_double2(mf.x * st, mf.y * st) : mf;
-    else w = diag ? mf : make_double2(mf.x * ist, mf.y * ist);
-    return make_double2(sg * w.x, sg * w.y);
+    const V mf = diag ? cm(u[e * N + a], u[c * N + a]) : cadd(cm(u[e * N + a], u[c * N + b]), cm(u[e * N + b], u[c * N + a]));
+    V w;
+    if (e < c) w = diag ? mk(mf.x * st, mf.y * st) : mf;
+    else w = diag ? mf : mk(mf.x * ist, mf.y * ist);
+    return mk(sg * w.x, sg * w.y);
   } else {
-    const double2 mf = csub(cm(u[e * N + a], u[c * N + b]), cm(u[e * N + b], u[c * N + a]));
-    return make_double2(-sg * mf.x, -sg * mf.y);
+    const V mf = csub(cm(u[e * N + a], u[c * N + b]), cm(u[e * N + b], u[c * N + a]));
+    return mk(-sg * mf.x, -sg * mf.y);
   }
 }
 
 // c0 = U^R h0, c1 = U^R h1 (DAG: U^R+) with U^R built from the fundamental link
 // at `site` of the planes Ug (plane stride `plane`)
-template <int FR, bool DAG>
-__device__ __forceinline__ void two_idx_mul2(double2 *c0, double2 *c1, const double2 *h0, const double2 *h1,
-                                             const double2 *Ug, long plane, long site, double sg) {
+template <int FR, bool DAG, typename V>
+__device__ __forceinline__ void two_idx_mul2(V *c0, V *c1, const V *h0, const V *h1, const V *Ug, long plane, long site,
+                                             decltype(V::x) sg) {
   constexpr int N = TwoIdx<FR>::NG;
-  double2 u[N * N];
+  V u[N * N];
 #pragma unroll
   for (int k = 0; k < N * N; k++) u[k] = ld_c(Ug + (long)k * plane + site);
 #pragma unroll
   for (int i = 0; i < 6; i++) {
-    double2 a0 = make_double2(0.0, 0.0), a1 = make_double2(0.0, 0.0);
+    V a0 = cmk<V>(0.0, 0.0), a1 = cmk<V>(0.0, 0.0);
 #pragma unroll
     for (int j = 0; j < 6; j++) {
       if (!DAG) {
-        const double2 v = two_idx_elem<FR>(u, i, j, sg);
+        const V v = two_idx_elem<FR>(u, i, j, sg);
         cmac(a0, v, h0[j]);
         cmac(a1, v, h1[j]);
       } else {
-        const double2 v = two_idx_elem<FR>(u, j, i, sg);
+        const V v = two_idx_elem<FR>(u, j, i, sg);
         cmacc(a0, v, h0[j]);
         cmacc(a1, v, h1[j]);
       }
@@ -427,9 +434,10 @@ __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb, co
           if (mu == 3) { h0[i] = caddi(s0, s2); h1[i] = csubi(s1, s3); }
         }
         if constexpr (FR != 0) {
-          const double sgr = (a.recon == 4 && mu == 0 && t == 0) ? -1.0 : 1.0;
-          two_idx_mul2<FR, false>(c0, c1, h0, h1, a.Ug + (long)mu * TwoIdx<FR>::NG * TwoIdx<FR>::NG * lplane, lplane,
-                                  so, sgr);
+          const R sgr = (a.recon == 4 && mu == 0 && t == 0) ? (R)-1 : (R)1;
+          two_idx_mul2<FR, false>(c0, c1, h0, h1,
+                                  (const V *)a.Ug + (long)mu * TwoIdx<FR>::NG * TwoIdx<FR>::NG * lplane, lplane, so,
+                                  sgr);
         } else {
           const R sgf = (a.recon == 2 && mu == 0 && t == 0) ? (R)-1 : (R)1;
           link_mul2<NA, false, R12, R12R>(c0, c1, h0, h1, Umu, lplane, so, nf, sgf);
@@ -461,9 +469,10 @@ __device__ __forceinline__ double hop_site(const HopArgs<R> &a, const int cb, co
         }
         const long sn = (long)inp * g.ld + cdn;
         if constexpr (FR != 0) {
-          const double sgr = (a.recon == 4 && mu == 0 && tm == 0) ? -1.0 : 1.0;
-          two_idx_mul2<FR, true>(c0, c1, h0, h1, a.Ug + (long)mu * TwoIdx<FR>::NG * TwoIdx<FR>::NG * lplane, lplane,
-                                 sn, sgr);
+          const R sgr = (a.recon == 4 && mu == 0 && tm == 0) ? (R)-1 : (R)1;
+          two_idx_mul2<FR, true>(c0, c1, h0, h1,
+                                 (const V *)a.Ug + (long)mu * TwoIdx<FR>::NG * TwoIdx<FR>::NG * lplane, lplane, sn,
+                                 sgr);
         } else {
           const R sgb = (a.recon == 2 && mu == 0 && tm == 0) ? (R)-1 : (R)1;
           link_mul2<NA, true, R12, R12R>(c0, c1, h0, h1, Umu, lplane, sn, nf, sgb);
@@ -537,7 +546,7 @@ __device__ __forceinline__ void pdl_enter() {
 }
 
 // RC: rebuild row 2 of the 3x3 links (instantiated for NF = 3 only); FR: build
-// the NF = 6 two-index links from the fundamental ones (FP64, see TwoIdx)
+// the NF = 6 two-index links from the fundamental ones (see TwoIdx)
 template <int NFT, bool REAL, typename R, int EP, int MINB, typename LE = typename LinkE<REAL, R>::T, bool RC = false,
           int FR = 0>
 __global__ void __launch_bounds__(HOP_THREADS, MINB) k_hop(HopArgs<R> a) {

@@ -80,12 +80,13 @@ static inline void (*hop_kernel(int recon))(HopArgs<R>) {
 }
 
 // variant 6: k_hop (variant 0's register budget) building the NF = 6
-// two-index links from the fundamental ones, FP64, while the fundamental links
-// are those the represented field was made from (link modes 3 and 4); -1 otherwise
+// two-index links from the fundamental ones (FP64 from L.Ug, FP32 from its
+// float copy L.Ugf) while the fundamental links are those the represented
+// field was made from (link modes 3 and 4); -1 otherwise
 template <int N, bool RL, typename R, int EP>
 int launch_fund(HopArgs<R> &a, dim3 grid, dim3 block, cudaStream_t s) {
-  if constexpr (N == 6 && !RL && sizeof(R) == 8) {
-    if (a.recon < 3) return -1;
+  if constexpr (N == 6 && !RL) {
+    if (a.recon < 3 || !a.Ug) return -1;
     if (L.repr == HRGPU_SYM)
       HR_CUDA(launch_pdl<R>(k_hop<N, RL, R, EP, 1, typename LinkE<RL, R>::T, false, 1>, grid, block, 0, s, a));
     else

@@ -64,6 +64,7 @@ struct Lattice {
   // gauge fields
   void *U = nullptr;      // represented links, double (double2 or double)
   void *Uf = nullptr;     // represented links, float
+  float2 *Ugf = nullptr;  // fundamental links, float (for the FP32 hop of link modes 3 and 4)
   double2 *Ug = nullptr;  // fundamental links [4][ng*ng][2*ld]
   bool have_gauge = false, have_gauge_flt = false, have_fund = false;
   // clover

@@ -63,7 +63,7 @@ static void free_ptr(void *p) {
 
 static void free_all() {
   cg_release();
-  void *ptrs[] = {L.d_h2d, L.d_d2h, L.U, L.Uf, L.Ubf, L.Ug, L.mom, L.cl_term, L.cl_dg, L.cl_od, L.cl_idg, L.cl_iod,
+  void *ptrs[] = {L.d_h2d, L.d_d2h, L.U, L.Uf, L.Ubf, L.Ug, L.Ugf, L.mom, L.cl_term, L.cl_dg, L.cl_od, L.cl_idg, L.cl_iod,
                   L.cl_dg_f, L.cl_idg_f, L.cl_od_f, L.cl_iod_f, L.cl_ldet, L.force_sum, L.cl_force, L.d_proj_off,
                   L.d_proj_k, L.d_proj_c, L.d_projk_off, L.d_projk_A, L.d_projk_c, L.partials, L.d_scalars, L.tmp_o, L.tmp_e, L.tmp_e2, L.tmp_full,
                   L.tmp_full2, L.tmp_o_f, L.tmp_e_f, L.tmp_full_f, L.stage, L.hop_err, L.hopb_err};
@@ -631,6 +631,12 @@ int hrgpu_assign_ud2u_f(void) {
   if (!L.Uf) HR_CUDA(cudaMalloc(&L.Uf, n * sizeof(float)));
   k_convert<float, double><<<nblk(n), 256, 0, L.stream>>>((float *)L.Uf, (const double *)L.U, n);
   HR_LAUNCH_CHECK();
+  if (L.recon12 >= 3) {  // the FP32 hop may build its links from these (variant 6)
+    const long ng = (long)4 * L.ng * L.ng * 2 * L.ld * 2;
+    if (!L.Ugf) HR_CUDA(cudaMalloc(&L.Ugf, ng * sizeof(float)));
+    k_convert<float, double><<<nblk(ng), 256, 0, L.stream>>>((float *)L.Ugf, (const double *)L.Ug, ng);
+    HR_LAUNCH_CHECK();
+  }
   L.have_gauge_flt = true;
   L.gauge_gen++;  // every write of the double links is followed by this call
   return 0;

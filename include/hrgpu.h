@@ -100,7 +100,7 @@ int hrgpu_represent_gauge_field(int bc_t_antiperiodic);
  * single-field hopping kernels load rows 0 and 1 only and rebuild row 2.
  * hrgpu_gauge_set_f runs the same check, trying the antiperiodic sign first.
  * The SU(3) symmetric and SU(4) antisymmetric representations (NF = 6): after
- * represent_gauge_field the FP64 single-field hopping kernel of variant 6 may
+ * represent_gauge_field the single-field hopping kernel of variant 6 may
  * build each represented link from the fundamental one (9 or 16 complex
  * numbers read instead of 36), until the fundamental links are written again
  * (hrgpu_gauge_set, update_gauge_field, project_gauge_field,
@@ -163,8 +163,9 @@ int hrgpu_g5Dphi_eopre_sq_flt(double m0, void *out, const void *in);
  * with the time halo staged in shared memory by bulk (TMA) copies (4 and 5: NF <= 4
  * complex, NF = 3 real; 5 also needs time slabs of a multiple of 128 sites per
  * parity), 6 = one thread per site building the SU(3) symmetric or SU(4)
- * antisymmetric links from the fundamental ones (FP64, link modes 3 and 4 of
- * hrgpu_link_recon), -1 = autotune on first use (default).  hrgpu_hop_tuning
+ * antisymmetric links from the fundamental ones (link modes 3 and 4 of
+ * hrgpu_link_recon; the FP32 operators from a float copy of the fundamental
+ * links made with the FP32 represented ones), -1 = autotune on first use (default).  hrgpu_hop_tuning
  * reports the variant chosen for (precision, epilogue 0..2) and the per-launch
  * times it measured (ms has room for 7 values; -1 marks a variant not built for
  * this NF, lattice or link mode); precision 2 is the FP32 operator reading BF16

@@ -1,6 +1,6 @@
 """The NF = 6 two-index representations (SU(3) symmetric, SU(4) antisymmetric)
-with the FP64 hopping kernels building each represented link from the
-fundamental one (link modes 3 and 4): every even-odd operator against the oracle
+with the hopping kernels building each represented link from the fundamental
+one (link modes 3 and 4; FP64, and FP32 from a float copy): every even-odd operator against the oracle
 and against the kernels that read the stored represented links, for both
 boundary conditions, with and without a clover term, and the rule that the mode
 ends as soon as the fundamental links are written without a new
@@ -75,6 +75,39 @@ def test_links_from_fundamental_match_oracle(bc, ng, rep):
             lat.Cphi_eopre(m, out, fe)
     finally:
         G._check(lat.L.hrgpu_set_link_recon(1), "set_link_recon")
+        G._check(lat.L.hrgpu_set_hop_variant(-1), "set_hop_variant")
+
+
+@pytest.mark.parametrize("bc", [True, False])
+@pytest.mark.parametrize("ng,rep", [(3, O.SYM), (4, O.ASYM)])
+def test_links_from_fundamental_fp32(bc, ng, rep):
+    """The FP32 operators with variant 6 (the links built in FP32 from a float copy
+    of the fundamental links) against the oracle's FP32 operators and against
+    variant 0 reading the stored FP32 links, within the FP32 tolerance."""
+    o, u, lat = make(ng, rep, bc)
+    m = -0.2
+    e = F.gaussian_spinor(5, o.VH, o.nf).astype(np.complex64)
+    fe, out = lat.field(O.EVEN, G.FLOAT, host=e), lat.field(O.EVEN, G.FLOAT)
+    try:
+        got = {}
+        for v in (6, 0):
+            G._check(lat.L.hrgpu_set_hop_variant(v), "set_hop_variant")
+            for name in ("Dphi_eopre_flt", "g5Dphi_eopre_flt", "g5Dphi_eopre_sq_flt"):
+                getattr(lat, name)(m, out, fe)
+                got[(v, name)] = out.download()
+        for name in ("Dphi_eopre_flt", "g5Dphi_eopre_flt", "g5Dphi_eopre_sq_flt"):
+            assert rel(got[(6, name)], getattr(o, name)(m, e)) < 2e-5, name
+            assert rel(got[(6, name)], got[(0, name)]) < 2e-6, name
+        o.clover_init(1.0)
+        o.compute_clover_term()
+        lat.clover_init(1.0)
+        for v in (6, 0):
+            G._check(lat.L.hrgpu_set_hop_variant(v), "set_hop_variant")
+            lat.g5Cphi_eopre_flt(m, out, fe)
+            got[(v, "c")] = out.download()
+        assert rel(got[(6, "c")], got[(0, "c")]) < 2e-6
+        assert rel(got[(6, "c")].astype(complex), o.g5Cphi_eopre(m, e.astype(complex))) < 2e-5
+    finally:
         G._check(lat.L.hrgpu_set_hop_variant(-1), "set_hop_variant")
 
 
