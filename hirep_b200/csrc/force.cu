@@ -247,9 +247,15 @@ __device__ __forceinline__ void prefetch_l2(const void *p) {
 // and the spinor at x (prefetch.global.L2, no registers held), so that their
 // loads, issued a few at a time after the neighbour's, wait for L2 rather than
 // for DRAM.
-template <int N, bool REAL, int E, bool PF>
-__global__ void __launch_bounds__(128, 4) k_force_hop_w3(double *fsum, const void *U, const double2 *X,
-                                                         const double2 *Y, Geo g, int dimg, double coeff) {
+//
+// FR (NF = 6 two-index representations, link modes 3 and 4): the link is
+// built from the fundamental one (Ug, 9 or 16 complex numbers) as the hop's
+// variant 6 does (two_idx_elem), with the antiperiodic sign when frbc is set;
+// the register budget is that of 3 blocks per SM.
+template <int N, bool REAL, int E, bool PF, int FR = 0>
+__global__ void __launch_bounds__(128, FR ? 3 : 4) k_force_hop_w3(double *fsum, const void *U, const double2 *X,
+                                                                  const double2 *Y, Geo g, int dimg, double coeff,
+                                                                  const double2 *Ug = nullptr, int frbc = 0) {
   extern __shared__ double hs[];  // [dimg][128]: this lane's generator sums in column tid
   const int tid = threadIdx.x, w = tid >> 5, h = w & 1;
   const long d0 = (long)(blockIdx.x >> 2) * 64 + (w >> 1) * 32 + (tid & 31);
@@ -283,20 +289,39 @@ __global__ void __launch_bounds__(128, 4) k_force_hop_w3(double *fsum, const voi
     if (mu == 3) { pt = caddi(a0, a2); pt2 = csubi(a1, a3); }
   }
   double2 ua[2][N];
+  if constexpr (FR != 0) {
+    static_assert(N == 6 && !REAL, "FR: the NF = 6 two-index representations");
+    constexpr int NG = TwoIdx<FR>::NG;
+    double2 fu[NG * NG];
 #pragma unroll
-  for (int i = 0; i < N; i++) {
-    ua[0][i] = ua[1][i] = make_double2(0, 0);
+    for (int k = 0; k < NG * NG; k++) fu[k] = __ldg(Ug + ((long)mu * NG * NG + k) * lp + d);
+    const double sg = (frbc && mu == 0 && t == 0) ? -1.0 : 1.0;
 #pragma unroll
-    for (int j = 0; j < N; j++) {
-      const long idx = ((long)mu * N * N + i * N + j) * lp + d;
-      if (REAL) {
-        const double u = ((const double *)U)[idx];
-        rmac(ua[0][i], u, a[0][j]);
-        rmac(ua[1][i], u, a[1][j]);
-      } else {
-        const double2 u = ((const double2 *)U)[idx];
+    for (int i = 0; i < N; i++) {
+      ua[0][i] = ua[1][i] = make_double2(0, 0);
+#pragma unroll
+      for (int j = 0; j < N; j++) {
+        const double2 u = two_idx_elem<FR>(fu, i, j, sg);
         cmac(ua[0][i], u, a[0][j]);
         cmac(ua[1][i], u, a[1][j]);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+      ua[0][i] = ua[1][i] = make_double2(0, 0);
+#pragma unroll
+      for (int j = 0; j < N; j++) {
+        const long idx = ((long)mu * N * N + i * N + j) * lp + d;
+        if (REAL) {
+          const double u = ((const double *)U)[idx];
+          rmac(ua[0][i], u, a[0][j]);
+          rmac(ua[1][i], u, a[1][j]);
+        } else {
+          const double2 u = ((const double2 *)U)[idx];
+          cmac(ua[0][i], u, a[0][j]);
+          cmac(ua[1][i], u, a[1][j]);
+        }
       }
     }
   }
@@ -680,11 +705,16 @@ __global__ void k_force_logdet(double2 *clf, const double *idg, const double2 *i
     }
 }
 
-template <int N, bool REAL, int E>
+template <int N, bool REAL, int E, int FR = 0>
 static void launch_force_w3(double *fsum, const void *U, const double2 *X, const double2 *Y, Geo g, int dimg,
                             double coeff, size_t smem, bool pf) {
   const unsigned grid = 4 * nb(2L * g.ld, 64);
-  if (pf) {
+  if constexpr (FR != 0) {
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(k_force_hop_w3<N, REAL, E, false, FR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_force_hop_w3<N, REAL, E, false, FR><<<grid, 128, smem, L.stream>>>(fsum, U, X, Y, g, dimg, coeff, L.Ug,
+                                                                           L.recon12 == 4);
+  } else if (pf) {
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(k_force_hop_w3<N, REAL, E, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_force_hop_w3<N, REAL, E, true><<<grid, 128, smem, L.stream>>>(fsum, U, X, Y, g, dimg, coeff);
@@ -696,13 +726,31 @@ static void launch_force_w3(double *fsum, const void *U, const double2 *X, const
 }
 
 // variant 1: one lane per link (k_force_hop_w); 2: two lanes per link in two
-// warps with the constant table (k_force_hop_w3); 3: 2 with the L2 prefetches.
-// Variants 2 and 3 need the padded table (ft_E > 0); without it variant 1 runs.
+// warps with the constant table (k_force_hop_w3); 3: 2 with the L2 prefetches;
+// 4: 2 with the NF = 6 two-index links built from the fundamental ones (link
+// modes 3 and 4; elsewhere variant 2).  Variants 2-4 need the padded table
+// (ft_E > 0); without it variant 1 runs.
 template <int N, bool REAL>
 static void launch_force_w(double *fsum, const void *U, const double2 *X, const double2 *Y, Geo g, ProjTabK P,
                            double coeff, size_t smem, int variant) {
   if constexpr ((!REAL && N <= 6) || (REAL && N == 3)) {
     if (variant >= 2 && ft_E > 0) {
+      if constexpr (N == 6 && !REAL) {
+        if (variant == 4 && L.recon_allow && L.recon12 >= 3 && L.Ug) {
+          const bool sym = L.repr == HRGPU_SYM;
+          if (ft_E == 2) {
+            if (sym) launch_force_w3<N, REAL, 2, 1>(fsum, U, X, Y, g, P.dimg, coeff, smem, false);
+            else launch_force_w3<N, REAL, 2, 2>(fsum, U, X, Y, g, P.dimg, coeff, smem, false);
+          } else if (ft_E == 3) {
+            if (sym) launch_force_w3<N, REAL, 3, 1>(fsum, U, X, Y, g, P.dimg, coeff, smem, false);
+            else launch_force_w3<N, REAL, 3, 2>(fsum, U, X, Y, g, P.dimg, coeff, smem, false);
+          } else {
+            if (sym) launch_force_w3<N, REAL, 5, 1>(fsum, U, X, Y, g, P.dimg, coeff, smem, false);
+            else launch_force_w3<N, REAL, 5, 2>(fsum, U, X, Y, g, P.dimg, coeff, smem, false);
+          }
+          return;
+        }
+      }
       const bool pf = variant == 3;
       if (ft_E == 2) launch_force_w3<N, REAL, 2>(fsum, U, X, Y, g, P.dimg, coeff, smem, pf);
       else if (ft_E == 3) launch_force_w3<N, REAL, 3>(fsum, U, X, Y, g, P.dimg, coeff, smem, pf);
@@ -814,7 +862,7 @@ int hrgpu_force_fermion_core(void *Xs, void *Ys, int auto_fill_odd, double dt, d
 }
 
 int hrgpu_set_force_variant(int variant) {
-  HR_REQUIRE(variant >= 0 && variant <= 3, HRGPU_E_ARG, "set_force_variant: variant must be 0..3");
+  HR_REQUIRE(variant >= 0 && variant <= 4, HRGPU_E_ARG, "set_force_variant: variant must be 0..4");
   L.force_variant = variant;
   return 0;
 }

@@ -439,8 +439,10 @@ int hrgpu_force_clover_logdet(double mass, double residue); /* force_fermion_cor
 /* kernel of the hopping part of force_fermion_core for complex NF <= 6 and real
  * NF = 3: 1 = one thread per link; 2 = two threads per link in two warps (one
  * per pairing of X and Y) with the algebra projection from a constant-memory
- * table; 3 = 2 with the link and the spinor at x prefetched into L2; 0 = the
- * default (2).  A tuning control of this library; it has no counterpart in
+ * table; 3 = 2 with the link and the spinor at x prefetched into L2; 4 = 2
+ * building the SU(3) symmetric or SU(4) antisymmetric links from the
+ * fundamental ones (link modes 3 and 4 of hrgpu_link_recon; elsewhere 2); 0 =
+ * the default (2).  A tuning control of this library; it has no counterpart in
  * the reference. */
 int hrgpu_set_force_variant(int variant);
 /* fermion_force_end (force_fermion_core.c:964-993): clover derivative, then adds the
