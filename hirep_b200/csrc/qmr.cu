@@ -112,7 +112,9 @@ __device__ __forceinline__ double q_g5(long e, int ld, int nf) {
   return ((int)((e / ld) % (4 * nf)) / nf) < 2 ? 1.0 : -1.0;
 }
 
-// Mp -= s_0 p2 (the shift of the first system, g5QMR_mshift.c:128); partials of <g5 p2, Mp>
+// Mp -= s_0 p2 (the shift of the first system, g5QMR_mshift.c:128); partials of
+// <g5 p2, Mp>.  SHIFT false: s_0 = 0 (the host knows the shifts), Mp is only read.
+template <bool SHIFT>
 __global__ void __launch_bounds__(RED_THREADS) k_q_alpha(const QMRState *S, double2 *Mp, const double2 *p2, long n,
                                                          int ld, int nf, double *partials) {
   if (S->state != 0) return;
@@ -122,8 +124,10 @@ __global__ void __launch_bounds__(RED_THREADS) k_q_alpha(const QMRState *S, doub
   for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
     const double2 a = p2[e];
     double2 v = Mp[e];
-    rmac(v, -s0, a);
-    Mp[e] = v;
+    if (SHIFT) {
+      rmac(v, -s0, a);
+      Mp[e] = v;
+    }
     acc += q_g5(e, ld, nf) * (a.x * v.x + a.y * v.y);
   }
   acc = block_sum(acc);
@@ -349,8 +353,12 @@ static int g5qmr_core(short *valid, int op, double mass, int n, const double *sh
       rc = apply_op(op, HRGPU_DOUBLE, mass, P[imp], P[ip2]);
       if (rc) break;
       per_it = mvm_count() - mb;
-      k_q_alpha<<<g, RED_THREADS, 0, L.stream>>>(QW.S, (double2 *)P[imp], (const double2 *)P[ip2], ne, L.ld, L.nf,
-                                                 L.partials);
+      if (shift[0] != 0.0)
+        k_q_alpha<true><<<g, RED_THREADS, 0, L.stream>>>(QW.S, (double2 *)P[imp], (const double2 *)P[ip2], ne, L.ld,
+                                                         L.nf, L.partials);
+      else
+        k_q_alpha<false><<<g, RED_THREADS, 0, L.stream>>>(QW.S, (double2 *)P[imp], (const double2 *)P[ip2], ne, L.ld,
+                                                          L.nf, L.partials);
       k_q_fold_alpha<<<1, RED_THREADS, 0, L.stream>>>(QW.S, L.partials, g);
       k_q_p<<<g, RED_THREADS, 0, L.stream>>>(QW.S, (double2 *)P[imp], (const double2 *)P[ip1],
                                              (const double2 *)P[ip2], ne, L.ld, L.nf, L.partials);
