@@ -878,7 +878,7 @@ def run_batch_solves(torch, stream, G, F):
     out["speedup_batch_fp64_vs_sequential_fp64"] = out["sequential_fp64_ms"] / out["batch_fp64_ms"]
     for q in (G.DOUBLE, G.FLOAT):
         for ep in (1, 2):
-            ch, tms = G.ctypes.c_int(), (G.ctypes.c_float * 5)()
+            ch, tms = G.ctypes.c_int(), (G.ctypes.c_float * 6)()
             lat.L.hrgpu_batch_tuning(q, ep, 12, G.ctypes.byref(ch), tms)
             out[f"tuning_{'f64' if q == G.DOUBLE else 'f32'}_ep{ep}_nb12"] = [ch.value] + [round(t, 4) for t in tms]
     return out

@@ -66,11 +66,12 @@ int launch_batch_tc(TileArgs<R> &a, int variant) {
   }
 }
 
-// variants: the register budget for 1, 3 or 4 resident blocks of 128 threads per SM
+// variants: the register budget for 1, 3 or 4 resident blocks of 128 threads per SM; 5:
+// the budget of 1 block with the link products in packed FP32 FMAs (complex FP32)
 template <typename R, int EP>
 int launch_batch_variant(TileArgs<R> &a, int variant) {
   a.g = make_geo();
-  if (variant >= 3) return launch_batch_tc<R, EP>(a, variant);
+  if (variant == 3 || variant == 4) return launch_batch_tc<R, EP>(a, variant);
   // 32 threads per (group of 8 sites, tile)
   const long threads = ((L.VH + TILE_S - 1) / TILE_S) * 32L * ((a.nb + TILE_F - 1) / TILE_F);
   dim3 grid((unsigned)((threads + HOPT_THREADS - 1) / HOPT_THREADS)), block(HOPT_THREADS);
@@ -80,6 +81,13 @@ int launch_batch_variant(TileArgs<R> &a, int variant) {
     switch (variant) {                                                     \
       case 0: k_hopt<N, RL, R, EP, 1><<<grid, block, 0, s>>>(a); break;     \
       case 1: k_hopt<N, RL, R, EP, 3><<<grid, block, 0, s>>>(a); break;     \
+      case 5:                                                              \
+        if constexpr (!RL && sizeof(R) == 4) {                             \
+          k_hopt<N, RL, R, EP, 1, true><<<grid, block, 0, s>>>(a);         \
+          break;                                                           \
+        } else {                                                           \
+          return -1;                                                       \
+        }                                                                  \
       default: k_hopt<N, RL, R, EP, 4><<<grid, block, 0, s>>>(a); break;    \
     }                                                                      \
     break;
@@ -132,11 +140,16 @@ int launch_batch(TileArgs<R> &a) {
     // the events are destroyed on every way out of the loop
     auto tune = [&]() -> int {
       for (int cand = 0; cand < HOPB_VARIANTS; cand++) {
-        if (cand >= 3) {  // the tensor-core kernels run when pinned (hrgpu_set_batch_variant(3 or 4))
+        if (cand == 3 || cand == 4) {  // the tensor-core kernels run when pinned (hrgpu_set_batch_variant(3 or 4))
           L.hopb_tune_ms[pi][EP][a.nb][cand] = -1.0f;
           continue;
         }
-        if (int rc = launch_batch_variant<R, EP>(a, cand)) return rc;
+        const int rc0 = launch_batch_variant<R, EP>(a, cand);
+        if (rc0 < 0) {  // not built for this precision or representation
+          L.hopb_tune_ms[pi][EP][a.nb][cand] = -1.0f;
+          continue;
+        }
+        if (rc0) return rc0;
         HR_CUDA(cudaEventRecord(e0, L.stream));
         for (int r = 0; r < 3; r++)
           if (int rc = launch_batch_variant<R, EP>(a, cand)) return rc;

@@ -40,11 +40,65 @@ struct TileArgs {
   Geo g;
 };
 
+// Packed FP32 arithmetic (fma.rn.f32x2: two FP32 FMAs in one instruction).
+// A complex product u h is (Re u, Re u) (Re h, Im h) + (Im u, Im u) (-Im h, Re h);
+// summing P = sum (Re u, Re u) h and Q = sum (Im u, Im u) h separately, the row
+// of U h is (P.x - Q.y, P.y + Q.x) and that of U^+ h (P.x + Q.y, P.y - Q.x):
+// two packed FMAs per link element and half spinor instead of four.
+__device__ __forceinline__ unsigned long long pk2(float x, float y) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(x), "f"(y));
+  return r;
+}
+__device__ __forceinline__ float2 upk2(unsigned long long r) {
+  float2 v;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+  return v;
+}
+__device__ __forceinline__ unsigned long long ffma2(unsigned long long a, unsigned long long b, unsigned long long c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
+// c0 = U h0, c1 = U h1 (DAG: U^+) for complex FP32 links, packed FMAs
+template <int NA, bool DAG>
+__device__ __forceinline__ void link_mul2_f2(float2 *c0, float2 *c1, const float2 *h0, const float2 *h1, const float2 *U,
+                                             long plane) {
+  unsigned long long g0[NA], g1[NA];
+#pragma unroll
+  for (int j = 0; j < NA; j++) {
+    g0[j] = pk2(h0[j].x, h0[j].y);
+    g1[j] = pk2(h1[j].x, h1[j].y);
+  }
+#pragma unroll
+  for (int i = 0; i < NA; i++) {
+    unsigned long long p0 = 0ull, q0 = 0ull, p1 = 0ull, q1 = 0ull;
+#pragma unroll
+    for (int j = 0; j < NA; j++) {
+      const float2 u = ld_c(U + (long)(DAG ? j * NA + i : i * NA + j) * plane);
+      const unsigned long long ur = pk2(u.x, u.x), ui = pk2(u.y, u.y);
+      p0 = ffma2(ur, g0[j], p0);
+      q0 = ffma2(ui, g0[j], q0);
+      p1 = ffma2(ur, g1[j], p1);
+      q1 = ffma2(ui, g1[j], q1);
+    }
+    const float2 P0 = upk2(p0), Q0 = upk2(q0), P1 = upk2(p1), Q1 = upk2(q1);
+    if (!DAG) {
+      c0[i] = make_float2(P0.x - Q0.y, P0.y + Q0.x);
+      c1[i] = make_float2(P1.x - Q1.y, P1.y + Q1.x);
+    } else {
+      c0[i] = make_float2(P0.x + Q0.y, P0.y - Q0.x);
+      c1[i] = make_float2(P1.x + Q1.y, P1.y - Q1.x);
+    }
+  }
+}
+
 // one (site cb, field f) of the hop with the fused epilogues of k_hop.  The
 // eight directions are unrolled so that the loads of a direction are issued
 // together (a loop over directions, one direction's loads live at a time and
 // twice the resident warps, measured 1.65x slower at NF=6).
-template <int NFT, bool REAL, typename R, int EP>
+template <int NFT, bool REAL, typename R, int EP, bool F2 = false>
 __device__ __forceinline__ void hopt_site(const TileArgs<R> &a, const int cb, const int tile, const int lane) {
   typedef typename C2<R>::T V;
   typedef typename LinkE<REAL, R>::T E;
@@ -98,7 +152,10 @@ __device__ __forceinline__ void hopt_site(const TileArgs<R> &a, const int cb, co
         if (mu == 3) { h0[i] = csubi(s0, s2); h1[i] = caddi(s1, s3); }
       }
     }
-    if (!bw) {
+    if constexpr (F2) {
+      if (!bw) link_mul2_f2<NA, false>(c0, c1, h0, h1, ubase(outp, cb, mu), LSTEP);
+      else link_mul2_f2<NA, true>(c0, c1, h0, h1, ubase(inp, cn, mu), LSTEP);
+    } else if (!bw) {
       const E *Ub = ubase(outp, cb, mu);
       link_mul<NA, false>(c0, h0, Ub, LSTEP, 0L, nf);
       link_mul<NA, false>(c1, h1, Ub, LSTEP, 0L, nf);
@@ -195,7 +252,7 @@ __device__ __forceinline__ void hopt_site(const TileArgs<R> &a, const int cb, co
 // A warp is 8 consecutive sites x the 4 fields of one tile; the warps of all
 // tiles of the same 8 sites are adjacent, so the links and clover blocks of
 // those sites are read from DRAM once and then hit in L1/L2 for the other tiles.
-template <int NFT, bool REAL, typename R, int EP, int MINB>
+template <int NFT, bool REAL, typename R, int EP, int MINB, bool F2 = false>
 __global__ void __launch_bounds__(HOPT_THREADS, MINB) k_hopt(TileArgs<R> a) {
   if (a.stop && *a.stop) return;
   const long flat = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -207,7 +264,7 @@ __global__ void __launch_bounds__(HOPT_THREADS, MINB) k_hopt(TileArgs<R> a) {
   const int tile = (int)(w - group * ntile);
   const long cbl = group * TILE_S + s8;
   if (cbl >= a.g.VH || tile * TILE_F + lane >= a.nb) return;
-  hopt_site<NFT, REAL, R, EP>(a, (int)cbl, tile, lane);
+  hopt_site<NFT, REAL, R, EP, F2>(a, (int)cbl, tile, lane);
 }
 
 // ---------------------------------------------------------------------------

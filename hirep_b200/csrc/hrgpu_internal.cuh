@@ -49,7 +49,7 @@ constexpr int MAXNF = 64;
 constexpr int RED_THREADS = 256;
 constexpr int RED_MAX_BLOCKS = 1184;  // 8 x 148 SMs
 constexpr int HOP_VARIANTS = 7;
-constexpr int HOPB_VARIANTS = 5;   // batch hopping kernel variants (3, 4: tensor cores)
+constexpr int HOPB_VARIANTS = 6;   // batch hopping kernel variants (3, 4: tensor cores; 5: packed FP32 FMAs)
 constexpr int HOPB_MAXNB = 64;     // fields per batch
 
 struct Lattice {

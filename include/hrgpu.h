@@ -404,10 +404,11 @@ int hrgpu_apply_op_batch(int op, int prec, double mass, void *out, const void *i
  * on the tensor cores, tcgen05 kind::tf32 with three products for FP32
  * accuracy, FP32 and complex NF = 6 only, nb <= 32; 4: the same with the
  * neighbours prefetched into shared memory two sites ahead, nb <= 16; 3 and 4
- * run only when pinned): -1 (default) autotunes variants 0-2 per precision,
- * epilogue and nb at first use; hrgpu_batch_tuning reports the choice (-1: not
- * tuned yet) and the tuning times in ms (5 entries, -1 for a variant not
- * timed). */
+ * run only when pinned; 5: variant 0 with the link products in packed FP32 FMAs,
+ * complex representations in FP32 only): -1 (default) autotunes variants 0-2
+ * and 5 per precision, epilogue and nb at first use; hrgpu_batch_tuning reports
+ * the choice (-1: not tuned yet) and the tuning times in ms (6 entries, -1 for a
+ * variant not timed). */
 int hrgpu_set_batch_variant(int variant);
 int hrgpu_batch_tuning(int prec, int epilogue, int nb, int *chosen, float *ms);
 /* cg_mshift for many sources at once (op: g5Dphi_eopre_sq or g5Cphi_eopre_sq).

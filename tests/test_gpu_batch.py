@@ -242,17 +242,48 @@ def test_batch_variants(variant, ng, rep, clover):
         G._check(lat.L.hrgpu_set_batch_variant(-1), "set_batch_variant")
 
 
+@pytest.mark.parametrize("ng,rep,clover", [(3, O.FUND, True), (3, O.SYM, True), (4, O.ASYM, False), (2, O.FUND, False)])
+def test_batch_packed_fma_variant(ng, rep, clover):
+    """Variant 5, the link products in packed FP32 FMAs (fma.rn.f32x2), for the
+    complex representations in FP32: every field against the FP32 single-field
+    operator (2e-6) and the oracle's FP64 operator (1e-5); in FP64 and for the
+    real representations the variant is not built."""
+    o, lat = setup((4, 4, 4, 8), ng, rep, seed=17, clover=1.0 if clover else None)
+    G._check(lat.L.hrgpu_set_batch_variant(5), "set_batch_variant")
+    try:
+        m, nb = (-0.3 if clover else -0.1), 7
+        ops = OPS_C[1:] if clover else OPS_W
+        hs = [F.gaussian_spinor(90 + i, o.VH, o.nf) for i in range(nb)]
+        fs = [lat.field(O.EVEN, G.FLOAT, host=h.astype(np.complex64)) for h in hs]
+        bin_, bout = lat.batch(nb, G.FLOAT, fields=fs), lat.batch(nb, G.FLOAT)
+        outs = [lat.field(O.EVEN, G.FLOAT) for _ in range(nb)]
+        single = lat.field(O.EVEN, G.FLOAT)
+        for op, name in ops:
+            lat.apply_op_batch(op, m, bout, bin_)
+            bout.unpack(outs)
+            for f in (0, nb // 2, nb - 1):
+                getattr(lat, name + "_flt")(m, single, fs[f])
+                assert rel(outs[f].download(), single.download()) < 2e-6, (name, f)
+                assert rel(outs[f].download().astype(complex), getattr(o, name)(m, hs[f])) < 1e-5, (name, f)
+        b64i, b64o = lat.batch(nb), lat.batch(nb)
+        with pytest.raises(G.HRGPUError, match="not built"):
+            lat.apply_op_batch(ops[0][0], m, b64o, b64i)
+    finally:
+        G._check(lat.L.hrgpu_set_batch_variant(-1), "set_batch_variant")
+
+
 def test_batch_autotuner_reports_its_choice():
     o, lat = setup((4, 4, 4, 4), 3, O.FUND, seed=13, clover=1.0)
     nb = 7
     bi, bo = lat.batch(nb), lat.batch(nb)
     lat.apply_op_batch(G.OP_G5CPHI_EOPRE, -0.2, bo, bi)
     chosen = ctypes.c_int(-2)
-    ms = (ctypes.c_float * 5)()
+    ms = (ctypes.c_float * 6)()
     for ep in (1, 2):  # the two clover epilogues ran
         G._check(lat.L.hrgpu_batch_tuning(G.DOUBLE, ep, nb, ctypes.byref(chosen), ms), "batch_tuning")
         assert 0 <= chosen.value < 3
         assert all(t > 0 for t in ms[:3]) and ms[3] == ms[4] == -1.0  # the tensor-core variants run only when pinned
+        assert ms[5] == -1.0  # the packed-FMA variant is FP32 only
     G._check(lat.L.hrgpu_batch_tuning(G.FLOAT, 0, nb, ctypes.byref(chosen), ms), "batch_tuning")
     assert chosen.value == -1  # not tuned: never ran
 
