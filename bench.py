@@ -661,7 +661,7 @@ def run_force_check(torch, stream, G, F, fd=((4, 1e-3), (4, 1e-4), (32, 1e-5))):
     f64, _ = force()
     core_ms = float(np.median([force()[1] for _ in range(5)]))
     by_variant = {}
-    for v in (1, 2, 3, 4):  # the kernels of the hopping force (hrgpu_set_force_variant)
+    for v in (1, 2, 3, 4, 5, 6):  # the kernels of the hopping force (hrgpu_set_force_variant)
         G._check(lat.L.hrgpu_set_force_variant(v), "set_force_variant")
         fv, _ = force()
         by_variant[str(v)] = {"ms": float(np.median([force()[1] for _ in range(5)])),
@@ -705,8 +705,9 @@ def run_force_check(torch, stream, G, F, fd=((4, 1e-3), (4, 1e-4), (32, 1e-5))):
             "force_fermion_core_ms": core_ms, "fp64_solve_s": solve_s,
             "force_fermion_core_ms_by_variant": by_variant,
             "variants": "1: one thread per link; 2: two threads per link in two warps, projection table in "
-                        "constant memory (default); 3: 2 with L2 prefetches of the link and the spinor at x; "
-                        "4: 2 with the links built from the fundamental ones",
+                        "constant memory; 3: 2 with L2 prefetches of the link and the spinor at x; "
+                        "4: 2 with the links built from the fundamental ones; 5: 2 with the link staged in "
+                        "shared memory by cp.async (default); 6: 5 with the spinor at x staged too",
             "algorithmic_bytes": core_bytes + fill_bytes,
             "algorithmic_bytes_note": "X, Y, links and force planes (read + write) of the core, plus the two "
                                       "odd-site fill hops" + (" (fundamental links)" if fill_fund else ""),

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "dirac.cuh"
+#include "hop_async.cuh"
 
 namespace hrgpu {
 
@@ -252,23 +253,48 @@ __device__ __forceinline__ void prefetch_l2(const void *p) {
 // built from the fundamental one (Ug, 9 or 16 complex numbers) as the hop's
 // variant 6 does (two_idx_elem), with the antiperiodic sign when frbc is set;
 // the register budget is that of 3 blocks per SM.
-template <int N, bool REAL, int E, bool PF, int FR = 0>
-__global__ void __launch_bounds__(128, FR ? 3 : 4) k_force_hop_w3(double *fsum, const void *U, const double2 *X,
+//
+// ST (complex links): the operands at x are copied into shared memory with
+// cp.async at the start, so that they are in flight while the neighbour's
+// spinor is loaded and projected without holding registers: ST = 1 the link
+// (each of the two warps of a site copies half its elements, read by both
+// after a barrier), ST = 2 the link and the lane's spinor at x (its own
+// copies, read back after its own wait; the register budget of 2 blocks per
+// SM, which its shared memory allows).  Shared memory after the generator
+// sums: the link [N*N][64 sites], then (ST = 2) the spinors [4 warps][4N][32].
+template <int N, bool REAL, int E, bool PF, int FR = 0, int ST = 0>
+__global__ void __launch_bounds__(128, FR ? 3 : ST == 2 ? 2 : 4) k_force_hop_w3(double *fsum, const void *U, const double2 *X,
                                                                   const double2 *Y, Geo g, int dimg, double coeff,
                                                                   const double2 *Ug = nullptr, int frbc = 0) {
   extern __shared__ double hs[];  // [dimg][128]: this lane's generator sums in column tid
   const int tid = threadIdx.x, w = tid >> 5, h = w & 1;
-  const long d0 = (long)(blockIdx.x >> 2) * 64 + (w >> 1) * 32 + (tid & 31);
+  const int sl = (w >> 1) * 32 + (tid & 31);  // this lane's site in the block
+  const long d0 = (long)(blockIdx.x >> 2) * 64 + sl;
   const int mu = blockIdx.x & 3;
   const int p0 = d0 >= g.ld ? 1 : 0;
   const bool valid = d0 < 2L * g.ld && d0 - p0 * g.ld < g.VH;
   const long d = valid ? d0 : 0;
+  const long lp = 2L * g.ld;
+  const double2 *c2 = h ? X : Y, *c1 = h ? Y : X;
+  double2 *sU = (double2 *)(hs + (long)dimg * 128);
+  double2 *sC = sU + N * N * 64 + (long)w * 4 * N * 32 + (tid & 31);
+  if constexpr (ST != 0) {
+    static_assert(!REAL && FR == 0 && !PF, "ST: complex stored links");
+#pragma unroll
+    for (int k = 0; k < (N * N + 1) / 2; k++) {
+      const int e = 2 * k + h;
+      if (e < N * N) cp_async16(sU + e * 64 + sl, (const double2 *)U + ((long)mu * N * N + e) * lp + d);
+    }
+    if constexpr (ST == 2) {
+#pragma unroll
+      for (int c = 0; c < 4 * N; c++) cp_async16(sC + c * 32, sp_at(c1, d, c, g.ld, N));
+    }
+    cp_async_commit();
+  }
   for (int A = 0; A < dimg; A++) hs[A * 128 + tid] = 0.0;
   int t, x, y, z;
   dev_coords(g, (int)d, t, x, y, z);
   const long dy = nbr_index(g, t, x, y, z, mu, +1);
-  const long lp = 2L * g.ld;
-  const double2 *c2 = h ? X : Y, *c1 = h ? Y : X;
   if (PF) {
 #pragma unroll
     for (int e = 0; e < N * N; e++)
@@ -307,13 +333,21 @@ __global__ void __launch_bounds__(128, FR ? 3 : 4) k_force_hop_w3(double *fsum, 
       }
     }
   } else {
+    if constexpr (ST != 0) {
+      cp_async_wait<0>();
+      __syncthreads();
+    }
 #pragma unroll
     for (int i = 0; i < N; i++) {
       ua[0][i] = ua[1][i] = make_double2(0, 0);
 #pragma unroll
       for (int j = 0; j < N; j++) {
         const long idx = ((long)mu * N * N + i * N + j) * lp + d;
-        if (REAL) {
+        if constexpr (ST != 0) {
+          const double2 u = sU[(i * N + j) * 64 + sl];
+          cmac(ua[0][i], u, a[0][j]);
+          cmac(ua[1][i], u, a[1][j]);
+        } else if (REAL) {
           const double u = ((const double *)U)[idx];
           rmac(ua[0][i], u, a[0][j]);
           rmac(ua[1][i], u, a[1][j]);
@@ -328,8 +362,18 @@ __global__ void __launch_bounds__(128, FR ? 3 : 4) k_force_hop_w3(double *fsum, 
   double2 (&b)[2][N] = a;
 #pragma unroll
   for (int i = 0; i < N; i++) {
-    const double2 b0 = *sp_at(c1, d, i, g.ld, N), b1 = *sp_at(c1, d, N + i, g.ld, N);
-    const double2 b2 = *sp_at(c1, d, 2 * N + i, g.ld, N), b3 = *sp_at(c1, d, 3 * N + i, g.ld, N);
+    double2 b0, b1, b2, b3;
+    if constexpr (ST == 2) {
+      b0 = sC[i * 32];
+      b1 = sC[(N + i) * 32];
+      b2 = sC[(2 * N + i) * 32];
+      b3 = sC[(3 * N + i) * 32];
+    } else {
+      b0 = *sp_at(c1, d, i, g.ld, N);
+      b1 = *sp_at(c1, d, N + i, g.ld, N);
+      b2 = *sp_at(c1, d, 2 * N + i, g.ld, N);
+      b3 = *sp_at(c1, d, 3 * N + i, g.ld, N);
+    }
     double2 &p2 = b[0][i], &p3 = b[1][i];
     if (mu == 0) { p2 = csub(b0, b2); p3 = csub(b1, b3); }
     if (mu == 1) { p2 = csubi(b0, b3); p3 = csubi(b1, b2); }
@@ -707,8 +751,24 @@ __global__ void k_force_logdet(double2 *clf, const double *idg, const double2 *i
 
 template <int N, bool REAL, int E, int FR = 0>
 static void launch_force_w3(double *fsum, const void *U, const double2 *X, const double2 *Y, Geo g, int dimg,
-                            double coeff, size_t smem, bool pf) {
+                            double coeff, size_t smem, bool pf, int st = 0) {
   const unsigned grid = 4 * nb(2L * g.ld, 64);
+  if constexpr (!REAL && FR == 0) {
+    if (st != 0) {
+      // the staged link (and spinors) after the generator sums
+      smem += sizeof(double2) * N * N * 64 + (st == 2 ? sizeof(double2) * 4 * 4 * N * 32 : 0);
+      if (st == 1) {
+        cudaFuncSetAttribute(k_force_hop_w3<N, REAL, E, false, 0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        k_force_hop_w3<N, REAL, E, false, 0, 1><<<grid, 128, smem, L.stream>>>(fsum, U, X, Y, g, dimg, coeff);
+      } else {
+        cudaFuncSetAttribute(k_force_hop_w3<N, REAL, E, false, 0, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        k_force_hop_w3<N, REAL, E, false, 0, 2><<<grid, 128, smem, L.stream>>>(fsum, U, X, Y, g, dimg, coeff);
+      }
+      return;
+    }
+  }
   if constexpr (FR != 0) {
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(k_force_hop_w3<N, REAL, E, false, FR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -728,8 +788,10 @@ static void launch_force_w3(double *fsum, const void *U, const double2 *X, const
 // variant 1: one lane per link (k_force_hop_w); 2: two lanes per link in two
 // warps with the constant table (k_force_hop_w3); 3: 2 with the L2 prefetches;
 // 4: 2 with the NF = 6 two-index links built from the fundamental ones (link
-// modes 3 and 4; elsewhere variant 2).  Variants 2-4 need the padded table
-// (ft_E > 0); without it variant 1 runs.
+// modes 3 and 4; elsewhere variant 2); 5: 2 with the link staged in shared
+// memory by cp.async (the default for complex links); 6: 5 with the spinor at
+// x staged too (5 and 6: complex links; real ones run 2).  Variants 2-6 need
+// the padded table (ft_E > 0); without it variant 1 runs.
 template <int N, bool REAL>
 static void launch_force_w(double *fsum, const void *U, const double2 *X, const double2 *Y, Geo g, ProjTabK P,
                            double coeff, size_t smem, int variant) {
@@ -752,9 +814,10 @@ static void launch_force_w(double *fsum, const void *U, const double2 *X, const 
         }
       }
       const bool pf = variant == 3;
-      if (ft_E == 2) launch_force_w3<N, REAL, 2>(fsum, U, X, Y, g, P.dimg, coeff, smem, pf);
-      else if (ft_E == 3) launch_force_w3<N, REAL, 3>(fsum, U, X, Y, g, P.dimg, coeff, smem, pf);
-      else launch_force_w3<N, REAL, 5>(fsum, U, X, Y, g, P.dimg, coeff, smem, pf);
+      const int st = variant == 5 ? 1 : variant == 6 ? 2 : 0;
+      if (ft_E == 2) launch_force_w3<N, REAL, 2>(fsum, U, X, Y, g, P.dimg, coeff, smem, pf, st);
+      else if (ft_E == 3) launch_force_w3<N, REAL, 3>(fsum, U, X, Y, g, P.dimg, coeff, smem, pf, st);
+      else launch_force_w3<N, REAL, 5>(fsum, U, X, Y, g, P.dimg, coeff, smem, pf, st);
     } else {
       if (smem > 48 * 1024)
         cudaFuncSetAttribute(k_force_hop_w<N, REAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -852,7 +915,7 @@ int hrgpu_force_fermion_core(void *Xs, void *Ys, int auto_fill_odd, double dt, d
     P.dimg = L.dimg;
     const size_t smem = sizeof(double) * 128 * L.dimg;
     if (int rc = force_table_upload()) return rc;
-    const int variant = L.force_variant ? L.force_variant : 2;
+    const int variant = L.force_variant ? L.force_variant : (L.real ? 2 : 5);
     HR_NF_DISPATCH(L.real, L.nf, (launch_force_w<N_, R_>(L.force_sum, L.U, X, Y, g, P, coeff, smem, variant)));
   } else {
     HR_NF_DISPATCH(L.real, L.nf, (k_force_hop<N_, R_><<<dim3(nb(n), 4), 128, 0, L.stream>>>(L.force_sum, L.U, X, Y, g, proj(), coeff)));
@@ -862,7 +925,7 @@ int hrgpu_force_fermion_core(void *Xs, void *Ys, int auto_fill_odd, double dt, d
 }
 
 int hrgpu_set_force_variant(int variant) {
-  HR_REQUIRE(variant >= 0 && variant <= 4, HRGPU_E_ARG, "set_force_variant: variant must be 0..4");
+  HR_REQUIRE(variant >= 0 && variant <= 6, HRGPU_E_ARG, "set_force_variant: variant must be 0..6");
   L.force_variant = variant;
   return 0;
 }

@@ -442,9 +442,11 @@ int hrgpu_force_clover_logdet(double mass, double residue); /* force_fermion_cor
  * per pairing of X and Y) with the algebra projection from a constant-memory
  * table; 3 = 2 with the link and the spinor at x prefetched into L2; 4 = 2
  * building the SU(3) symmetric or SU(4) antisymmetric links from the
- * fundamental ones (link modes 3 and 4 of hrgpu_link_recon; elsewhere 2); 0 =
- * the default (2).  A tuning control of this library; it has no counterpart in
- * the reference. */
+ * fundamental ones (link modes 3 and 4 of hrgpu_link_recon; elsewhere 2); 5 =
+ * 2 with the link staged in shared memory by cp.async; 6 = 5 with the spinor
+ * at x staged too (5 and 6: complex links; real ones run 2); 0 = the default
+ * (5 for complex links, 2 for real ones).  A tuning control of this library;
+ * it has no counterpart in the reference. */
 int hrgpu_set_force_variant(int variant);
 /* fermion_force_end (force_fermion_core.c:964-993): clover derivative, then adds the
  * accumulated force to the host momentum field force[V][4][NG*NG-1] (HiRep layout) */

@@ -302,14 +302,15 @@ def test_force_matches_oracle(ng, rep, clover):
     assert rel(fg - mom, fo - mom) < 1e-12
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("ng,rep", [(2, O.FUND), (3, O.FUND), (2, O.ADJ), (4, O.ASYM), (3, O.SYM), (4, O.FUND),
                                     (5, O.FUND), (6, O.FUND)])
 def test_force_variants(variant, ng, rep):
     """Every kernel of the hopping force (one lane per link; two lanes per link in two
     warps with the constant-memory projection table, padded to 2, 3 or 5 entries per
-    element, without and with L2 prefetches, and with the NF = 6 two-index links
-    built from the fundamental ones) gives the oracle's force, on a
+    element, without and with L2 prefetches, with the NF = 6 two-index links
+    built from the fundamental ones, and with the link, or the link and the
+    spinor at x, staged in shared memory by cp.async) gives the oracle's force, on a
     4x6x6x6 lattice whose half volume (432) is not a multiple of 32, so the last
     block holds padding sites that compute and write nothing."""
     o, lat, _, _ = setup((4, 6, 6, 6), ng, rep, seed=19, smooth=0.3, gpu_represent=True)
