@@ -59,6 +59,29 @@ template <typename V> __device__ __forceinline__ V ld_c(const V *p) { return __l
 __device__ __forceinline__ double ld_c(const double *p) { return __ldg(p); }
 __device__ __forceinline__ float ld_c(const float *p) { return __ldg(p); }
 
+// read-only loads that do not allocate in L1: a single-field hop reads each
+// link once, so its links pass L1 by and leave it to the neighbour spinors
+__device__ __forceinline__ double2 ld_u(const double2 *p) {
+  double2 v;
+  asm("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float2 ld_u(const float2 *p) {
+  float2 v;
+  asm("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double ld_u(const double *p) {
+  double v;
+  asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float ld_u(const float *p) {
+  float v;
+  asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+
 // chi = U h (DAG=false) or U^+ h (DAG=true); U element (i,j) at U[(i*nf+j)*plane + site]
 template <int NA> struct Unroll { static constexpr int v = NA <= 12 ? NA : 1; };
 
@@ -143,7 +166,8 @@ __device__ __forceinline__ void link_mul(float2 *chi, const float2 *h, const __n
 // R12 (complex NF = 3 links stored in the operator's own precision, in the
 // kernels instantiated for reconstruction): only rows 0 and 1 are loaded and
 // row 2 is rebuilt as sg conj(r0 x r1) (su3_row2), a third less link traffic;
-// otherwise the full link is read.
+// otherwise the full link is read.  The link loads do not allocate in L1
+// (ld_u): a single-field hop reads each link once.
 // The real form (R12R: SU(2) adjoint links, SO(3)) rebuilds row 2 as sg (r0 x r1).
 template <int NA, bool DAG, bool R12, bool R12R = false, typename V, typename E, typename R>
 __device__ __forceinline__ void link_mul2(V *c0, V *c1, const V *h0, const V *h1, const E *U, long plane, long site,
@@ -151,7 +175,7 @@ __device__ __forceinline__ void link_mul2(V *c0, V *c1, const V *h0, const V *h1
   if constexpr (R12R) {
     R u[9];
 #pragma unroll
-    for (int e = 0; e < 6; e++) u[e] = ld_c(U + (long)e * plane + site);
+    for (int e = 0; e < 6; e++) u[e] = ld_u(U + (long)e * plane + site);
     so3_row2(u, sg);
 #pragma unroll
     for (int i = 0; i < 3; i++) {
@@ -171,7 +195,7 @@ __device__ __forceinline__ void link_mul2(V *c0, V *c1, const V *h0, const V *h1
     {
       V u[9];
 #pragma unroll
-      for (int e = 0; e < 6; e++) u[e] = ld_c(U + (long)e * plane + site);
+      for (int e = 0; e < 6; e++) u[e] = ld_u(U + (long)e * plane + site);
       su3_row2(u, sg);
 #pragma unroll
       for (int i = 0; i < 3; i++) {
@@ -192,8 +216,36 @@ __device__ __forceinline__ void link_mul2(V *c0, V *c1, const V *h0, const V *h1
       return;
     }
   }
-  link_mul<NA, DAG>(c0, h0, U, plane, site, nf);
-  link_mul<NA, DAG>(c1, h1, U, plane, site, nf);
+  if constexpr (std::is_same<E, __nv_bfloat162>::value || std::is_same<E, __nv_bfloat16>::value) {
+    link_mul<NA, DAG>(c0, h0, U, plane, site, nf);  // BF16 storage
+    link_mul<NA, DAG>(c1, h1, U, plane, site, nf);
+  } else {
+    // the full link, each element loaded once for both half spinors
+#pragma unroll
+    for (int i = 0; i < NA; i++) {
+      if (i >= nf) break;
+      V a0 = cmk<V>(0.0, 0.0), a1 = cmk<V>(0.0, 0.0);
+#pragma unroll (Unroll<NA>::v)
+      for (int j = 0; j < NA; j++) {
+        if (j >= nf) break;
+        const E u = ld_u(U + (long)(DAG ? j * nf + i : i * nf + j) * plane + site);
+        if constexpr (sizeof(E) == sizeof(V)) {
+          if (!DAG) {
+            cmac(a0, u, h0[j]);
+            cmac(a1, u, h1[j]);
+          } else {
+            cmacc(a0, u, h0[j]);
+            cmacc(a1, u, h1[j]);
+          }
+        } else {
+          rmac(a0, u, h0[j]);
+          rmac(a1, u, h1[j]);
+        }
+      }
+      c0[i] = a0;
+      c1[i] = a1;
+    }
+  }
 }
 
 // BF16 storage type of a link element
@@ -356,7 +408,7 @@ __device__ __forceinline__ void two_idx_mul2(V *c0, V *c1, const V *h0, const V 
   constexpr int N = TwoIdx<FR>::NG;
   V u[N * N];
 #pragma unroll
-  for (int k = 0; k < N * N; k++) u[k] = ld_c(Ug + (long)k * plane + site);
+  for (int k = 0; k < N * N; k++) u[k] = ld_u(Ug + (long)k * plane + site);
 #pragma unroll
   for (int i = 0; i < 6; i++) {
     V a0 = cmk<V>(0.0, 0.0), a1 = cmk<V>(0.0, 0.0);
