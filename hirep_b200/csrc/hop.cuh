@@ -82,6 +82,34 @@ __device__ __forceinline__ float ld_u(const float *p) {
   return v;
 }
 
+// read-once data (the clover blocks of a single-field hop): no L1 allocation
+// and first out of L2, so that the links and spinors the next hop reads stay
+__device__ __forceinline__ unsigned long long l2_evict_first() {
+  unsigned long long pol;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ double2 ld_ef(const double2 *p, unsigned long long pol) {
+  double2 v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float2 ld_ef(const float2 *p, unsigned long long pol) {
+  float2 v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;" : "=f"(v.x), "=f"(v.y) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double ld_ef(const double *p, unsigned long long pol) {
+  double v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float ld_ef(const float *p, unsigned long long pol) {
+  float v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  return v;
+}
+
 // chi = U h (DAG=false) or U^+ h (DAG=true); U element (i,j) at U[(i*nf+j)*plane + site]
 template <int NA> struct Unroll { static constexpr int v = NA <= 12 ? NA : 1; };
 
@@ -259,13 +287,15 @@ struct LinkBF16<true> {
 };
 
 // y = H x for one packed Hermitian 2NF x 2NF block (diag real, strict lower complex)
-template <int NA, typename V, typename R>
+// EF: the blocks are loaded with ld_ef (read once)
+template <int NA, bool EF = false, typename V, typename R>
 __device__ __forceinline__ void herm_apply(V *y, const V *x, const R *dg, const V *od, long plane, long site, int nf) {
   const int n = 2 * nf;
+  const unsigned long long pol = EF ? l2_evict_first() : 0ull;
 #pragma unroll
   for (int i = 0; i < 2 * NA; i++) {
     if (i >= n) break;
-    R d = ld_c(dg + (long)i * plane + site);
+    R d = EF ? ld_ef(dg + (long)i * plane + site, pol) : ld_c(dg + (long)i * plane + site);
     y[i] = cscale(d, x[i]);
   }
 #pragma unroll (Unroll<2 * NA>::v)
@@ -274,7 +304,8 @@ __device__ __forceinline__ void herm_apply(V *y, const V *x, const R *dg, const 
 #pragma unroll (Unroll<2 * NA>::v)
     for (int j = 0; j < 2 * NA; j++) {
       if (j >= i) break;
-      V l = ld_c(od + (long)(i * (i - 1) / 2 + j) * plane + site);
+      const V *pl = od + (long)(i * (i - 1) / 2 + j) * plane + site;
+      V l = EF ? ld_ef(pl, pol) : ld_c(pl);
       cmac(y[i], l, x[j]);   // y_i += L_ij x_j
       cmacc(y[j], l, x[i]);  // y_j += conj(L_ij) x_i
     }
@@ -320,7 +351,7 @@ __device__ __forceinline__ void clover_epilogue(V (&ra)[NA], V (&rb)[NA], const 
       xin[nf + i] = ld_c(aux + (long)((2 * b + 1) * nf + i) * cs);
     }
   }
-  herm_apply<NA>(yout, xin, a.cdg + (long)b * n2 * lp, a.cod + (long)b * no * lp, lp, site, nf);
+  herm_apply<NA, true>(yout, xin, a.cdg + (long)b * n2 * lp, a.cod + (long)b * no * lp, lp, site, nf);
 #pragma unroll
   for (int i = 0; i < NA; i++) {
     if (EP == EP_CLOV_INV) {
@@ -746,7 +777,7 @@ __device__ __forceinline__ double hop2_site(const HopArgs<R> &a, const int cb, c
         ch[i] = u1;
       }
     }
-    herm_apply<NA>(yout, xin, a.cdg + (long)h * n2 * lp, a.cod + (long)h * no * lp, lp, site, nf);
+    herm_apply<NA, true>(yout, xin, a.cdg + (long)h * n2 * lp, a.cod + (long)h * no * lp, lp, site, nf);
     const R sb = h ? sg : (R)1;
 #pragma unroll
     for (int i = 0; i < NA; i++) {
