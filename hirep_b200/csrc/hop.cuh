@@ -109,12 +109,43 @@ __device__ __forceinline__ float ld_ef(const float *p, unsigned long long pol) {
   asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
   return v;
 }
+// the same policy in L2 with the line kept in L1 (data that other warps of
+// the SM read again soon: the batched kernel's links and clover blocks)
+__device__ __forceinline__ double2 ld_ef1(const double2 *p, unsigned long long pol) {
+  double2 v;
+  asm("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float2 ld_ef1(const float2 *p, unsigned long long pol) {
+  float2 v;
+  asm("ld.global.nc.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;" : "=f"(v.x), "=f"(v.y) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double ld_ef1(const double *p, unsigned long long pol) {
+  double v;
+  asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float ld_ef1(const float *p, unsigned long long pol) {
+  float v;
+  asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  return v;
+}
+// load policy LP: 0 read-only (ld_c), 1 ld_ef, 2 ld_ef1
+template <int LP, typename T>
+__device__ __forceinline__ T ld_p(const T *p, unsigned long long pol) {
+  if constexpr (LP == 1) return ld_ef(p, pol);
+  else if constexpr (LP == 2) return ld_ef1(p, pol);
+  else return ld_c(p);
+}
 
 // chi = U h (DAG=false) or U^+ h (DAG=true); U element (i,j) at U[(i*nf+j)*plane + site]
 template <int NA> struct Unroll { static constexpr int v = NA <= 12 ? NA : 1; };
 
-template <int NA, bool DAG, typename V>
+// LP: load policy of the link elements (ld_p)
+template <int NA, bool DAG, int LP = 0, typename V>
 __device__ __forceinline__ void link_mul(V *chi, const V *h, const V *U, long plane, long site, int nf) {
+  const unsigned long long pol = LP ? l2_evict_first() : 0ull;
 #pragma unroll
   for (int i = 0; i < NA; i++) {
     if (i >= nf) break;
@@ -123,10 +154,10 @@ __device__ __forceinline__ void link_mul(V *chi, const V *h, const V *U, long pl
     for (int j = 0; j < NA; j++) {
       if (j >= nf) break;
       if (!DAG) {
-        V u = ld_c(U + (long)(i * nf + j) * plane + site);
+        V u = ld_p<LP>(U + (long)(i * nf + j) * plane + site, pol);
         cmac(a, u, h[j]);
       } else {
-        V u = ld_c(U + (long)(j * nf + i) * plane + site);
+        V u = ld_p<LP>(U + (long)(j * nf + i) * plane + site, pol);
         cmacc(a, u, h[j]);
       }
     }
@@ -134,8 +165,9 @@ __device__ __forceinline__ void link_mul(V *chi, const V *h, const V *U, long pl
   }
 }
 
-template <int NA, bool DAG, typename V, typename R>
+template <int NA, bool DAG, int LP = 0, typename V, typename R>
 __device__ __forceinline__ void link_mul(V *chi, const V *h, const R *U, long plane, long site, int nf) {
+  const unsigned long long pol = LP ? l2_evict_first() : 0ull;
 #pragma unroll
   for (int i = 0; i < NA; i++) {
     if (i >= nf) break;
@@ -143,7 +175,7 @@ __device__ __forceinline__ void link_mul(V *chi, const V *h, const R *U, long pl
 #pragma unroll (Unroll<NA>::v)
     for (int j = 0; j < NA; j++) {
       if (j >= nf) break;
-      R u = DAG ? ld_c(U + (long)(j * nf + i) * plane + site) : ld_c(U + (long)(i * nf + j) * plane + site);
+      R u = ld_p<LP>(U + (long)(DAG ? j * nf + i : i * nf + j) * plane + site, pol);
       rmac(a, u, h[j]);
     }
     chi[i] = a;
@@ -287,15 +319,15 @@ struct LinkBF16<true> {
 };
 
 // y = H x for one packed Hermitian 2NF x 2NF block (diag real, strict lower complex)
-// EF: the blocks are loaded with ld_ef (read once)
-template <int NA, bool EF = false, typename V, typename R>
+// LP: load policy of the blocks (ld_p; 1 for a single-field hop, which reads them once)
+template <int NA, int LP = 0, typename V, typename R>
 __device__ __forceinline__ void herm_apply(V *y, const V *x, const R *dg, const V *od, long plane, long site, int nf) {
   const int n = 2 * nf;
-  const unsigned long long pol = EF ? l2_evict_first() : 0ull;
+  const unsigned long long pol = LP ? l2_evict_first() : 0ull;
 #pragma unroll
   for (int i = 0; i < 2 * NA; i++) {
     if (i >= n) break;
-    R d = EF ? ld_ef(dg + (long)i * plane + site, pol) : ld_c(dg + (long)i * plane + site);
+    R d = ld_p<LP>(dg + (long)i * plane + site, pol);
     y[i] = cscale(d, x[i]);
   }
 #pragma unroll (Unroll<2 * NA>::v)
@@ -304,8 +336,7 @@ __device__ __forceinline__ void herm_apply(V *y, const V *x, const R *dg, const 
 #pragma unroll (Unroll<2 * NA>::v)
     for (int j = 0; j < 2 * NA; j++) {
       if (j >= i) break;
-      const V *pl = od + (long)(i * (i - 1) / 2 + j) * plane + site;
-      V l = EF ? ld_ef(pl, pol) : ld_c(pl);
+      V l = ld_p<LP>(od + (long)(i * (i - 1) / 2 + j) * plane + site, pol);
       cmac(y[i], l, x[j]);   // y_i += L_ij x_j
       cmacc(y[j], l, x[i]);  // y_j += conj(L_ij) x_i
     }
@@ -351,7 +382,7 @@ __device__ __forceinline__ void clover_epilogue(V (&ra)[NA], V (&rb)[NA], const 
       xin[nf + i] = ld_c(aux + (long)((2 * b + 1) * nf + i) * cs);
     }
   }
-  herm_apply<NA, true>(yout, xin, a.cdg + (long)b * n2 * lp, a.cod + (long)b * no * lp, lp, site, nf);
+  herm_apply<NA, 1>(yout, xin, a.cdg + (long)b * n2 * lp, a.cod + (long)b * no * lp, lp, site, nf);
 #pragma unroll
   for (int i = 0; i < NA; i++) {
     if (EP == EP_CLOV_INV) {
@@ -777,7 +808,7 @@ __device__ __forceinline__ double hop2_site(const HopArgs<R> &a, const int cb, c
         ch[i] = u1;
       }
     }
-    herm_apply<NA, true>(yout, xin, a.cdg + (long)h * n2 * lp, a.cod + (long)h * no * lp, lp, site, nf);
+    herm_apply<NA, 1>(yout, xin, a.cdg + (long)h * n2 * lp, a.cod + (long)h * no * lp, lp, site, nf);
     const R sb = h ? sg : (R)1;
 #pragma unroll
     for (int i = 0; i < NA; i++) {

@@ -65,6 +65,7 @@ __device__ __forceinline__ unsigned long long ffma2(unsigned long long a, unsign
 template <int NA, bool DAG>
 __device__ __forceinline__ void link_mul2_f2(float2 *c0, float2 *c1, const float2 *h0, const float2 *h1, const float2 *U,
                                              long plane) {
+  const unsigned long long pol = l2_evict_first();
   unsigned long long g0[NA], g1[NA];
 #pragma unroll
   for (int j = 0; j < NA; j++) {
@@ -76,7 +77,7 @@ __device__ __forceinline__ void link_mul2_f2(float2 *c0, float2 *c1, const float
     unsigned long long p0 = 0ull, q0 = 0ull, p1 = 0ull, q1 = 0ull;
 #pragma unroll
     for (int j = 0; j < NA; j++) {
-      const float2 u = ld_c(U + (long)(DAG ? j * NA + i : i * NA + j) * plane);
+      const float2 u = ld_ef1(U + (long)(DAG ? j * NA + i : i * NA + j) * plane, pol);
       const unsigned long long ur = pk2(u.x, u.x), ui = pk2(u.y, u.y);
       p0 = ffma2(ur, g0[j], p0);
       q0 = ffma2(ui, g0[j], q0);
@@ -157,12 +158,12 @@ __device__ __forceinline__ void hopt_site(const TileArgs<R> &a, const int cb, co
       else link_mul2_f2<NA, true>(c0, c1, h0, h1, ubase(inp, cn, mu), LSTEP);
     } else if (!bw) {
       const E *Ub = ubase(outp, cb, mu);
-      link_mul<NA, false>(c0, h0, Ub, LSTEP, 0L, nf);
-      link_mul<NA, false>(c1, h1, Ub, LSTEP, 0L, nf);
+      link_mul<NA, false, 2>(c0, h0, Ub, LSTEP, 0L, nf);
+      link_mul<NA, false, 2>(c1, h1, Ub, LSTEP, 0L, nf);
     } else {
       const E *Ub = ubase(inp, cn, mu);
-      link_mul<NA, true>(c0, h0, Ub, LSTEP, 0L, nf);
-      link_mul<NA, true>(c1, h1, Ub, LSTEP, 0L, nf);
+      link_mul<NA, true, 2>(c0, h0, Ub, LSTEP, 0L, nf);
+      link_mul<NA, true, 2>(c1, h1, Ub, LSTEP, 0L, nf);
     }
 #pragma unroll
     for (int i = 0; i < NA; i++) {
@@ -226,7 +227,7 @@ __device__ __forceinline__ void hopt_site(const TileArgs<R> &a, const int cb, co
       }
       const R *dg = a.cdg + ((blk * 2 + b) * N2) * LSTEP + (cb & 7);
       const V *od = a.cod + ((blk * 2 + b) * NO) * LSTEP + (cb & 7);
-      herm_apply<NA>(yout, xin, dg, od, LSTEP, 0L, nf);
+      herm_apply<NA, 2>(yout, xin, dg, od, LSTEP, 0L, nf);
 #pragma unroll
       for (int i = 0; i < NA; i++) {
         if (EP == EP_CLOV_INV) {
