@@ -379,7 +379,7 @@ def main():
         return max_over_ranks(float(np.mean(ts)), dist, "cuda")
 
     lat.set_host_chunks(args.host_chunks)
-    e2e_ms = time_e2e(e2e_pipelined, extra_warmup=8)  # the first 8 calls choose the form
+    e2e_ms = time_e2e(e2e_pipelined, extra_warmup=32)  # the first 32 calls choose the form
     e2e_seq_ms = time_e2e(e2e_sequential)
     form, ms_pipe, ms_seq = G.ctypes.c_int(), G.ctypes.c_float(), G.ctypes.c_float()
     G._check(lat.L.hrgpu_host_form(G.ctypes.byref(form), G.ctypes.byref(ms_pipe), G.ctypes.byref(ms_seq)),

@@ -42,8 +42,11 @@
 // is made for a new key, the plain sequence (one copy in, the operator on the
 // whole lattice, one copy out) is captured beside it, both are replayed and
 // timed on the spot, and the first calls for that key then alternate the two
-// and keep the one with the lower mean device time per call
-// (hrgpu_set_host_form pins one form, hrgpu_host_form reports the choice).
+// and keep the one with the lower median device time per call; the load on
+// the host's PCIe changes while a program runs, so the calls alternate the two
+// forms again every HP_RECHECK calls (hrgpu_set_host_form pins one form,
+// hrgpu_host_form reports the choice).
+#include <algorithm>
 #include <utility>
 #include <vector>
 
@@ -79,13 +82,15 @@ struct HostGraph {
   int v0, v1, flt_links, pdl;
   long VH;
   cudaGraphExec_t exec = nullptr;
-  // form 0 (auto): the other form's graph while the first calls try both
+  // form 0 (auto): the other form's graph, for the trial calls that try both
   cudaGraphExec_t alt = nullptr;
-  int trials = 0;
-  double tsum[2] = {0.0, 0.0};  // GPU time of the trial calls, by form (pipelined, sequential)
+  int trials = 0;    // trial calls made in the current round of trials
+  long calls = 0;    // calls since the last round of trials ended
+  float tt[2][16];   // GPU time of the trial calls, by form (pipelined, sequential)
   int tn[2] = {0, 0};
 };
-constexpr int HP_TRIALS = 8;  // calls that alternate the two forms before one is kept
+constexpr int HP_TRIALS = 32;     // calls that alternate the two forms before one is kept
+constexpr long HP_RECHECK = 1024;  // calls after which the two forms are tried again
 static std::vector<HostGraph> HG;  // a few cached graphs
 constexpr size_t HG_MAX = 8;
 
@@ -406,14 +411,19 @@ static int apply_host(int clover, int g5, double mass, void *host_out, const voi
       HG.push_back(key);
       hit = &HG.back();
     }
-    if (!hit->alt) {
+    if (hit->alt && hit->trials >= HP_TRIALS && ++hit->calls >= HP_RECHECK) {
+      hit->trials = 0;  // a new round of trials
+      hit->tn[0] = hit->tn[1] = 0;
+    }
+    if (!hit->alt || hit->trials >= HP_TRIALS) {
       HR_CUDA(cudaGraphLaunch(hit->exec, L.stream));
     } else {
       // The replays timed when the graphs were made run back to back; the calls
       // of a program come with host work between them, and on some hosts the
       // order of the two forms differs between the two patterns.  So the first
-      // HP_TRIALS calls alternate the forms, timed on the device, and the form
-      // with the lower mean is kept (the results are bit-identical).
+      // HP_TRIALS calls (and HP_TRIALS calls every HP_RECHECK calls after them)
+      // alternate the forms, timed on the device, and the form with the lower
+      // median is kept (the results are bit-identical).
       static cudaEvent_t te[2] = {nullptr, nullptr};
       if (!te[0]) {
         HR_CUDA(cudaEventCreate(&te[0]));
@@ -427,15 +437,17 @@ static int apply_host(int clover, int g5, double mass, void *host_out, const voi
       HR_CUDA(cudaStreamSynchronize(L.stream));
       float ms = 0;
       HR_CUDA(cudaEventElapsedTime(&ms, te[0], te[1]));
-      hit->tsum[f] += ms;
-      hit->tn[f]++;
+      if (hit->tn[f] < HP_TRIALS / 2) hit->tt[f][hit->tn[f]++] = ms;
       if (++hit->trials >= HP_TRIALS) {
-        const double m0 = hit->tsum[0] / hit->tn[0], m1 = hit->tsum[1] / hit->tn[1];
+        auto median = [](float *v, int n) {
+          std::sort(v, v + n);
+          return n % 2 ? (double)v[n / 2] : 0.5 * ((double)v[n / 2 - 1] + (double)v[n / 2]);
+        };
+        const double m0 = median(hit->tt[0], hit->tn[0]), m1 = median(hit->tt[1], hit->tn[1]);
         const int best = m1 < m0 ? FORM_SEQUENTIAL : FORM_PIPELINED;
         if (best != hit->form) std::swap(hit->exec, hit->alt);
-        cudaGraphExecDestroy(hit->alt);
-        hit->alt = nullptr;
         hit->form = best;
+        hit->calls = 0;
         hp_last_form = best;
         hp_last_ms[0] = (float)m0;
         hp_last_ms[1] = (float)m1;

@@ -212,14 +212,15 @@ int hrgpu_set_host_chunks(int chunks); /* chunks of the pipeline (default 10; 1 
 /* With pinned buffers the operator runs as a cached CUDA graph per (operator,
  * mass, buffers, ...).  Form 0 (default): when a graph is made, the pipelined
  * form and the plain sequence (one copy each way around the whole-lattice
- * operator) are both captured and timed, the faster is used first, the first 8
+ * operator) are both captured and timed, the faster is used first, the first 32
  * calls for that graph alternate the two (timed on the device) and the one with
- * the lower mean is kept; 1 forces the pipeline, 2 the plain sequence.  No
- * HiRep counterpart (host-field transport). */
+ * the lower median is kept, and 32 calls alternate them again after every 1024
+ * calls; 1 forces the pipeline, 2 the plain sequence.  No HiRep counterpart
+ * (host-field transport). */
 int hrgpu_set_host_form(int form);
 /* the form chosen for the last graph made (1 pipelined, 2 sequential, -1 none
  * yet) and the times behind the choice (ms: the replays when the graph was made,
- * then the trial calls' means once they are done; -1 if not timed) */
+ * then the trial calls' medians once a round of them is done; -1 if not timed) */
 int hrgpu_host_form(int *form, float *ms_pipelined, float *ms_sequential);
 
 /* ---------------------------------------------------------------- clover -- */
