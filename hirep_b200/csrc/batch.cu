@@ -985,14 +985,15 @@ int hrgpu_cg_mshift_batch(int op, double mass, int nsrc, const int *nshift, cons
     return status;
   }
 
-  // Defect correction (cg_mshift_flt.c:144-276).  Round 1 starts from x = 0,
-  // where the residuals of a source's shifts are all equal: as in HiRep, one
-  // FP32 multi-shift solve per source corrects all its shifts.  After an FP32
-  // inner solve the shifted residuals are collinear only to the FP32 noise
-  // (about 1e-2 of their size at an inner tolerance of 1e-5), so HiRep's
-  // projection onto the first residual gains two digits a round for the other
-  // shifts.  From round 2 on every unconverged system is therefore corrected
-  // from its own residual: one single-shift Krylov space each, all in one batch.
+  // Defect correction (cg_mshift_flt.c:144-276).  The first correction pass
+  // starts from x = 0, where the residuals of a source's shifts are all equal:
+  // as in HiRep, one FP32 multi-shift solve per source corrects all its shifts.
+  // After an FP32 inner solve the shifted residuals are collinear only to the
+  // FP32 noise (about 1e-2 of their size at an inner tolerance of 1e-5), so
+  // HiRep's projection onto the first residual gains two digits a pass for the
+  // other shifts.  From the second pass on every unconverged system is
+  // therefore corrected from its own residual: one single-shift Krylov space
+  // each, all in one batch.
   if (int rc = ensure_batch_buf(&BO.rhs, &BO.hrhs, batch_bytes(HRGPU_FLOAT, ns))) return rc;
   if (int rc = ensure_batch_buf(&BO.xf, &BO.hxf, batch_bytes(HRGPU_FLOAT, ns))) return rc;
   HR_CUDA(cudaMemsetAsync(BO.x, 0, batch_bytes(HRGPU_DOUBLE, ns), L.stream));
