@@ -263,9 +263,9 @@ __device__ __forceinline__ void prefetch_l2(const void *p) {
 // SM, which its shared memory allows).  Shared memory after the generator
 // sums: the link [N*N][64 sites], then (ST = 2) the spinors [4 warps][4N][32].
 template <int N, bool REAL, int E, bool PF, int FR = 0, int ST = 0>
-__global__ void __launch_bounds__(128, FR ? 3 : ST == 2 ? 2 : 4) k_force_hop_w3(double *fsum, const void *U, const double2 *X,
-                                                                  const double2 *Y, Geo g, int dimg, double coeff,
-                                                                  const double2 *Ug = nullptr, int frbc = 0) {
+__global__ void __launch_bounds__(128, FR ? 3 : ST == 2 ? 2 : 4)
+    k_force_hop_w3(double *fsum, const void *U, const double2 *X, const double2 *Y, Geo g, int dimg, double coeff,
+                   const double2 *Ug = nullptr, int frbc = 0) {
   extern __shared__ double hs[];  // [dimg][128]: this lane's generator sums in column tid
   const int tid = threadIdx.x, w = tid >> 5, h = w & 1;
   const int sl = (w >> 1) * 32 + (tid & 31);  // this lane's site in the block
