@@ -48,3 +48,26 @@ def test_errors_are_reported_not_fatal():
     rc = lib.hrgpu_geometry(0, 4, 4, 4, None, None, None)
     assert rc == 2
     assert b"bad arguments" in lib.hrgpu_last_error()
+
+
+@pytest.mark.parametrize("setter,good,bad,default", [
+    ("hrgpu_set_hop_variant", [-1, 0, 6], [-2, 7], -1),
+    ("hrgpu_set_batch_variant", [-1, 0, 5], [-2, 6], -1),
+    ("hrgpu_set_force_variant", [0, 5, 6], [-1, 7], 0),
+    ("hrgpu_set_host_form", [0, 1, 2], [-1, 3], 0),
+    ("hrgpu_set_host_chunks", [1, 10], [0, -3], 10),
+])
+def test_tuning_controls_check_their_arguments(setter, good, bad, default):
+    """The tuning controls are host state: each accepts its documented range and
+    refuses anything else with HRGPU_E_ARG (2) and a message naming the call,
+    without a GPU."""
+    lib = hrgpu.lib()
+    fn = getattr(lib, setter)
+    try:
+        for v in good:
+            assert fn(v) == 0
+        for v in bad:
+            assert fn(v) == 2
+            assert setter[len("hrgpu_"):].encode() in lib.hrgpu_last_error()
+    finally:
+        assert fn(default) == 0
